@@ -1,0 +1,1969 @@
+"""CUDA code generation for sm_100a (replaces sandbox/codegen.py and
+sandbox/targetc.py).
+
+For every pipeline this module emits one CUDA translation unit:
+
+* one kernel per fused stencil group (``GroupPlan``): a CTA per tile of the
+  group's anchor runs region inference for its tile, stages stencil inputs
+  into shared memory (TMA ``cp.async.bulk.tensor`` with an mbarrier when the
+  buffer is 16-byte aligned, cooperative loads otherwise), computes every
+  materialized stage over its region into shared memory in topological
+  order (cheap stages are evaluated in registers at their use points, with
+  common subexpressions shared), and writes live-outs to HBM for the points
+  the tile owns;
+* for a ``Reduction``: an init pass and a tiled accumulation kernel that
+  privatizes the tile's target footprint in shared memory and flushes it
+  with global atomics (the reference only supports ``+=``,
+  sandbox/codegen.py:268-295; Min/Max/Mul are supported here too);
+* for a ``const`` function: host C++ that tabulates it (compiled by the host
+  compiler with the reference's flags so the table is bit-identical to what
+  the reference's generated C++ computes) and an upload to HBM;
+* host code: parameter validation (the bounds checks, per call), a
+  workspace for intermediate arrays (storage_mapping.py), launches, and the
+  ``extern "C"`` entry points.
+
+Entry points of ``pipeline_<name>``, with the reference's argument order
+(parameters sorted by name, then inputs, then outputs:
+sandbox/codegen.py:957-1007, sandbox/targetc.py:344-366):
+
+* ``void pipeline_<name>(params..., void* in..., void* out...)`` -- host
+  buffers, synchronous: the reference's drop-in ABI.
+* ``int pipeline_<name>_dev(params..., void* in..., void* out...,
+  void* stream)`` -- device buffers, asynchronous on ``stream``.
+* ``int pipeline_<name>_batch(int n, const int* iparams,
+  const float* fparams, void* const* in, void* const* out, void* stream)``
+  -- many images (each with its own parameters) in one launch per group.
+* ``int pipeline_<name>_graph(params..., ptrs..., void* stream)`` -- replays
+  a CUDA graph of the whole pipeline captured on first use.
+* ``int pipeline_<name>_status(void)`` and ``int pipeline_<name>_check(void)``
+  -- last status, and the device error word (synchronizing).
+
+Semantics kept from the reference's C target: C integer arithmetic and
+promotion, truncating ``/`` and ``%``, stores convert to the stage's
+element type (also for stages computed in registers), ``Select`` evaluates
+both arms.  Float literals are emitted as ``float`` on the device (the
+reference prints them as double, sandbox/targetc.py:80-86; the difference
+is inside the stated tolerance) and exactly as the reference prints them in
+host code for const tables.  Points of a stage not covered by any ``Case``
+read as 0 (a defined value for what the reference leaves uninitialized);
+points of a pipeline output not covered by any ``Case`` are left untouched,
+as in the reference.
+"""
+
+import re
+
+from . import constructs as C
+from .expr_ast import (Value, AbstractBinaryOpNode, AbstractUnaryOpNode,
+                       InbuiltFunction)
+from .expression import substitute_vars, getType, affine_form
+from .bounds import part_boxes
+from .pipe import body_parts
+from .tiling import IndexFn, is_data_dependent
+from .evaluate import monotone_dir
+
+_INT_T = (C.Int, C.UInt, C.Short, C.UShort, C.Char, C.UChar, C.Long,
+          C.ULong)
+
+
+class CodegenError(Exception):
+    pass
+
+
+class CudaModule(object):
+    """Generated sources of one pipeline."""
+
+    def __init__(self, name, source, host_source, header, meta):
+        self.name = name
+        self.source = source
+        self.host_source = host_source
+        self.header = header
+        self.meta = meta
+
+    def __str__(self):
+        return self.source
+
+
+class W(object):
+    """Indented line writer."""
+
+    def __init__(self):
+        self.lines = []
+        self.ind = 0
+
+    def __call__(self, s=""):
+        for line in s.split("\n"):
+            self.lines.append(("  " * self.ind + line) if line else "")
+
+    def open(self, s):
+        self(s + " {")
+        self.ind += 1
+
+    def close(self, s="}"):
+        self.ind -= 1
+        self(s)
+
+    def text(self):
+        return "\n".join(self.lines) + "\n"
+
+
+def ctype(t):
+    if t not in _INT_T and t not in (C.Float, C.Double):
+        raise CodegenError("no C type for %s" % t)
+    return t.c_decl()
+
+
+def _float_lit(v, suffix):
+    v = float(v)
+    if v != v or v in (float('inf'), float('-inf')):
+        raise CodegenError("non-finite literal")
+    s = repr(v)
+    if 'e' not in s and '.' not in s:
+        s += '.0'
+    return s + suffix
+
+
+# ---------------------------------------------------------------------------
+class Names(object):
+    def __init__(self):
+        self.used = {}
+        self.of = {}
+
+    def get(self, obj, base):
+        if id(obj) in self.of:
+            return self.of[id(obj)]
+        b = re.sub(r'[^A-Za-z0-9_]', '_', base)
+        n = b
+        i = 1
+        while n in self.used:
+            i += 1
+            n = "%s_%d" % (b, i)
+        self.used[n] = obj
+        self.of[id(obj)] = n
+        return n
+
+
+class ExprCtx(object):
+    """Expression printer with scoped common-subexpression temps.
+
+    ``reader(func, arg_asts)`` returns a C lvalue/expression for a producer
+    value (a shared-memory or global read, or an inlined computation) and
+    may emit statements; ``bind`` maps DSL variables to ASTs over the loop
+    variables of the point being computed."""
+
+    def __init__(self, w, mode, params, reader):
+        self.w = w
+        self.mode = mode              # 'device' | 'host'
+        self.params = params          # Parameter -> C name
+        self.reader = reader
+        self.scopes = [{}]
+        self.ntemp = 0
+
+    def temp(self):
+        self.ntemp += 1
+        return "t%d" % self.ntemp
+
+    def lookup(self, key):
+        for s in reversed(self.scopes):
+            if key in s:
+                return s[key]
+        return None
+
+    def define(self, key, name):
+        self.scopes[-1][key] = name
+
+    def push(self):
+        self.scopes.append({})
+
+    def pop(self):
+        self.scopes.pop()
+
+    # ---- printing ----------------------------------------------------------
+    def lit(self, v):
+        t = v.typ
+        x = v.value
+        if t is C.Rational:
+            if x.denominator == 1:
+                return str(int(x))
+            return "(%s)" % _float_lit(float(x), '' if self.mode == 'host'
+                                       else 'f')
+        if t in _INT_T:
+            x = int(x)
+            s = str(x)
+            if abs(x) >= (1 << 31):
+                s += "LL"
+            return "(%s)" % s if x < 0 else s
+        if t is C.Float:
+            s = _float_lit(x, '' if self.mode == 'host' else 'f')
+        else:
+            s = _float_lit(x, '')
+        return "(%s)" % s if s.startswith('-') else s
+
+    def expr(self, e, bind):
+        e = Value.numericToValue(e)
+        if isinstance(e, Value):
+            return self.lit(e)
+        if isinstance(e, C.Parameter):
+            if e not in self.params:
+                raise CodegenError("unknown parameter %s" % e.name)
+            return self.params[e]
+        if isinstance(e, C.Variable):
+            if e in bind:
+                b = bind[e]
+                if isinstance(b, str):
+                    return b
+                return self.expr(b, {})
+            if hasattr(e, '_cname'):
+                return e._cname
+            raise CodegenError("unbound variable %s" % e.name)
+        if isinstance(e, C.Reference):
+            args = [_subst(a, bind) for a in e.arguments]
+            return self.reader(e.objectRef, args, self)
+        if isinstance(e, AbstractBinaryOpNode):
+            return "(%s %s %s)" % (self.expr(e.left, bind), e.op,
+                                   self.expr(e.right, bind))
+        if isinstance(e, AbstractUnaryOpNode):
+            return "(%s%s)" % (e.op, self.expr(e.child, bind))
+        if isinstance(e, C.Cast):
+            return "((%s)(%s))" % (ctype(e.typ), self.expr(e.expression, bind))
+        if isinstance(e, C.Select):
+            c = self.cond(e.condition, bind)
+            a = self.expr(e.true_expression, bind)
+            b = self.expr(e.false_expression, bind)
+            return "(%s ? %s : %s)" % (c, a, b)
+        if isinstance(e, InbuiltFunction):
+            args = ", ".join(self.expr(a, bind) for a in e.arguments)
+            return "%s(%s)" % (self._fname(e), args)
+        raise CodegenError("cannot print %r" % (e,))
+
+    def _fname(self, e):
+        if isinstance(e, C.RandomFloat):
+            raise CodegenError("RandomFloat is not supported")
+        if self.mode == 'host':
+            return {C.Pow: 'pow', C.Powf: 'powf', C.Log: 'log',
+                    C.Exp: 'std::exp', C.Sin: 'std::sin', C.Cos: 'std::cos',
+                    C.Sqrt: 'std::sqrt', C.Sqrtf: 'sqrtf',
+                    C.Abs: 'std::abs'}[type(e)]
+        return {C.Pow: 'pow', C.Powf: 'powf', C.Log: 'log', C.Exp: 'exp',
+                C.Sin: 'sin', C.Cos: 'cos', C.Sqrt: 'sqrt', C.Sqrtf: 'sqrtf',
+                C.Abs: 'pm_abs'}[type(e)]
+
+    def cond(self, c, bind):
+        op = c.conditional
+        if op in ('&&', '||'):
+            return "(%s %s %s)" % (self.cond(c.lhs, bind), op,
+                                   self.cond(c.rhs, bind))
+        return "(%s %s %s)" % (self.expr(c.lhs, bind), op,
+                               self.expr(c.rhs, bind))
+
+    def index(self, e):
+        """Canonical C text of an index AST over loop variables."""
+        f = affine_form(e)
+        if f is not None:
+            parts = []
+            for k, c in sorted(f[0].items(), key=lambda kv: self.expr(
+                    kv[0], {})):
+                n = self.expr(k, {})
+                if c == 1:
+                    parts.append(n)
+                elif c == -1:
+                    parts.append("-" + n)
+                else:
+                    parts.append("%d*%s" % (c, n))
+            if f[1] or not parts:
+                parts.append(str(f[1]))
+            s = " + ".join(parts).replace("+ -", "- ")
+            return "(%s)" % s
+        return self.expr(e, {})
+
+
+def _vn(v):
+    return "v_" + re.sub(r'[^A-Za-z0-9_]', '_', v.name)
+
+
+def _subst(a, bind):
+    """Substitute a variable binding (values are ASTs) into an index AST."""
+    if not bind:
+        return a
+    m = dict((k, v) for k, v in bind.items() if not isinstance(v, str))
+    if not m:
+        return a
+    return substitute_vars(a, m)
+
+
+def _loop_vars(n, prefix="q"):
+    vs = []
+    for i in range(n):
+        v = C.Variable(C.Int, "%s%d" % (prefix, i))
+        v._cname = "%s%d" % (prefix, i)
+        vs.append(v)
+    return vs
+
+
+# ---------------------------------------------------------------------------
+class PipelineGen(object):
+    def __init__(self, pipeline):
+        self.p = pipeline
+        self.names = Names()
+        self.pname = re.sub(r'[^A-Za-z0-9_]', '_', pipeline.name)
+        self.params, self.inputs, self.outputs = pipeline.ordered_params()
+        self.pmap = {}
+        for prm in self.params:
+            self.pmap[prm] = "p_" + self.names.get(prm, prm.name)
+        self.iparams = [q for q in self.params
+                        if q.typ not in (C.Float, C.Double)]
+        self.fparams = [q for q in self.params
+                        if q.typ in (C.Float, C.Double)]
+        self.fname = {}
+        all_funcs = list(self.inputs) + [c.func for c in pipeline.comps]
+        for f in all_funcs:
+            self.fname[id(f)] = self.names.get(f, f.name)
+        self.w = W()
+        self.hw = W()                 # host .cpp for const tables
+        self.kernels = []
+        self.meta = {'groups': []}
+
+    def fn(self, f):
+        return self.fname[id(f)]
+
+    def ptype(self, prm):
+        return 'float' if prm in self.fparams else 'int'
+
+    # ---- expressions common to kernels and host ---------------------------
+    def dom_exprs(self, f, ctx):
+        out = []
+        for d in f.domain:
+            out.append((ctx.expr(d.lowerBound, {}), ctx.expr(d.upperBound,
+                                                            {})))
+        return out
+
+    def declare_params(self, w, src):
+        for prm in self.params:
+            w("const %s %s = %s.%s;" % (self.ptype(prm), self.pmap[prm], src,
+                                        self.pmap[prm]))
+
+    def declare_domain(self, w, f, ctx, need_strides):
+        n = self.fn(f)
+        dom = self.dom_exprs(f, ctx)
+        for d, (lo, hi) in enumerate(dom):
+            w("const int d_%s_lo%d = %s, d_%s_hi%d = %s;" % (n, d, lo, n, d,
+                                                            hi))
+        if need_strides:
+            nd = len(dom)
+            w("const long long s_%s_%d = 1;" % (n, nd - 1))
+            for d in range(nd - 2, -1, -1):
+                w("const long long s_%s_%d = s_%s_%d * (long long)"
+                  "(d_%s_hi%d - d_%s_lo%d + 1);" % (n, d, n, d + 1, n, d + 1,
+                                                    n, d + 1))
+
+    def gindex(self, f, args, ctx, clamp_dd=True):
+        """Linear index into a dense array of ``f`` at index ASTs ``args``;
+        data-dependent components are clamped into the domain."""
+        n = self.fn(f)
+        terms = []
+        nd = len(args)
+        for d, a in enumerate(args):
+            s = ctx.index(a)
+            if clamp_dd and is_data_dependent(a):
+                s = "pm_clampi(%s, d_%s_lo%d, d_%s_hi%d)" % (s, n, d, n, d)
+            if d == nd - 1:
+                terms.append("(long long)(%s - d_%s_lo%d)" % (s, n, d))
+            else:
+                terms.append("(long long)(%s - d_%s_lo%d) * s_%s_%d" % (
+                    s, n, d, n, d))
+        return " + ".join(terms)
+
+    def host_text(self):
+        if not self.hw.lines:
+            return None
+        return ("// const tables of pipeline %s -- generated by polymage_b200"
+                "\n#include <cmath>\n#include <cstdlib>\n#include <cstring>"
+                "\n#define isl_min(x,y) ((x) < (y) ? (x) : (y))\n"
+                "#define isl_max(x,y) ((x) > (y) ? (x) : (y))\n"
+                "static inline int pm_clampi(int v, int lo, int hi) "
+                "{ return v < lo ? lo : (v > hi ? hi : v); }\n" %
+                self.p.name) + self.hw.text()
+
+    def gen_args_struct(self):
+        w = self.w
+        w.open("struct pm_args")
+        for prm in self.params:
+            w("%s %s;" % (self.ptype(prm), self.pmap[prm]))
+        for f in self.inputs + self.outputs:
+            w("void* b_%s;" % self.fn(f))
+        w("char* ws;")
+        w("char* ctab;")
+        w.close("};")
+        w("")
+
+    # ---- per-call validation ------------------------------------------------
+    def gen_validate(self):
+        w = self.w
+        ctx = ExprCtx(w, 'device', self.pmap, None)
+        w("// Bounds checks of the spec, repeated for this call's parameters")
+        w("// (a call whose references would leave a producer's domain is")
+        w("// refused instead of reading out of bounds).")
+        w.open("static int pm_validate(const pm_args& A)")
+        self.declare_params(w, "A")
+        for f in self.inputs + self.outputs:
+            for d, (lo, hi) in enumerate(self.dom_exprs(f, ctx)):
+                w("if ((long long)(%s) - (long long)(%s) + 1 < 0) "
+                  "return PM_ERR_PARAMS;" % (hi, lo))
+        checks = getattr(self.p, '_bounds_checks', [])
+        seen = set()
+        for (comp, box, arg, g, dim, is_target) in checks:
+            key = (id(comp), id(box), str(arg), id(g), dim)
+            if key in seen:
+                continue
+            seen.add(key)
+            vs = [v for v in arg.collect(C.Variable)
+                  if not isinstance(v, C.Parameter)]
+            w.open("")
+            ok = True
+            for v in box.variables:
+                los = [ctx.expr(e, {}) for e in box.lo[v]]
+                his = [ctx.expr(e, {}) for e in box.hi[v]]
+                lo = los[0]
+                for x in los[1:]:
+                    lo = "isl_max_i(%s, %s)" % (lo, x)
+                hi = his[0]
+                for x in his[1:]:
+                    hi = "isl_min_i(%s, %s)" % (hi, x)
+                w("const int %s_lo = %s, %s_hi = %s;" % (_vn(v), lo, _vn(v),
+                                                          hi))
+            empt = " || ".join("%s_lo > %s_hi" % (_vn(v), _vn(v))
+                               for v in box.variables)
+            w("bool empty = %s;" % (empt or "false"))
+            lo_b = {}
+            hi_b = {}
+            for v in vs:
+                dd = monotone_dir(arg, v)
+                if dd is None:
+                    ok = False
+                    break
+                if dd >= 0:
+                    lo_b[v], hi_b[v] = _vn(v) + "_lo", _vn(v) + "_hi"
+                else:
+                    lo_b[v], hi_b[v] = _vn(v) + "_hi", _vn(v) + "_lo"
+            if ok:
+                glo = ctx.expr(g.domain[dim].lowerBound, {})
+                ghi = ctx.expr(g.domain[dim].upperBound, {})
+                a_lo = ctx.expr(arg, lo_b)
+                a_hi = ctx.expr(arg, hi_b)
+                w("if (!empty && ((%s) < (%s) || (%s) > (%s))) return "
+                  "PM_ERR_PARAMS;" % (a_lo, glo, a_hi, ghi))
+            w.close()
+        w("return PM_OK;")
+        w.close()
+        w("")
+
+    # ---- workspace layout -----------------------------------------------------
+    def gen_workspace(self):
+        w = self.w
+        ctx = ExprCtx(w, 'device', self.pmap, None)
+        slots = getattr(self.p, '_storage_slots', [])
+        self.slot_of = getattr(self.p, '_storage_assign', {})
+        w("// Intermediate arrays: one slot per storage class occupant chain,")
+        w("// sized per call (bytes = max over the slot's occupants).")
+        w.open("static void pm_ws_layout(const pm_args& A, size_t* off, "
+               "size_t* total)")
+        self.declare_params(w, "A")
+        w("size_t o = 0;")
+        for i, occ in enumerate(slots):
+            w("{ size_t b = 0;")
+            for comp in occ:
+                f = comp.func
+                ext = " * ".join("(size_t)pm_nonneg((%s) - (%s) + 1)" % (
+                    ctx.expr(d.upperBound, {}), ctx.expr(d.lowerBound, {}))
+                    for d in f.domain)
+                w("  { size_t e = (size_t)%d * %s; if (e > b) b = e; }" % (
+                    f.typ.size(), ext))
+            w("  off[%d] = o; o += pm_align256(b); }" % i)
+        w("*total = o;")
+        w.close()
+        w("")
+        self.nslots = len(slots)
+
+    def buf_expr(self, f, src="A"):
+        """C expression of the device pointer of a full array."""
+        if any(f is x for x in self.inputs + self.outputs):
+            return "%s.b_%s" % (src, self.fn(f))
+        comp = self.p.func_map.get(f)
+        if comp is not None and comp in self.slot_of:
+            return "(%s.ws + wsoff[%d])" % (src, self.slot_of[comp])
+        if f.is_const_func:
+            return "ctab_ptr_%s" % self.fn(f)
+        raise CodegenError("no buffer for %s" % f.name)
+
+    # ---- entry points -----------------------------------------------------------
+    def abi_params(self):
+        ps = ["%s %s" % (self.ptype(q), q.name) for q in self.params]
+        ps += ["void* %s" % f.name for f in self.inputs]
+        ps += ["void* %s" % f.name for f in self.outputs]
+        return ps
+
+    def gen_entries(self):
+        w = self.w
+        name = self.pname
+        launches = self.launch_fns
+        ctx = ExprCtx(w, 'device', self.pmap, None)
+        w("static pm_arena pm_ws_arena;")
+        w("static pm_arena pm_ctab_arena;")
+        w("")
+        # ---- single image, device pointers ----
+        w.open("static int pm_run(pm_args& A, cudaStream_t s)")
+        w("int st = pm_validate(A);")
+        w("if (st) return st;")
+        w("size_t wsoff[%d + 1]; size_t wstotal = 0;" % max(self.nslots, 1))
+        w("pm_ws_layout(A, wsoff, &wstotal);")
+        w("void* ws = nullptr;")
+        w("if ((st = pm_arena_get(&pm_ws_arena, wstotal, &ws))) return st;")
+        w("A.ws = (char*)ws;")
+        for fnm in launches:
+            w("if ((st = %s(A, wsoff, s))) return st;" % fnm)
+        w("return PM_OK;")
+        w.close()
+        w("")
+        sig = ", ".join(self.abi_params())
+        call_fill = []
+        for q in self.params:
+            call_fill.append("A.%s = %s;" % (self.pmap[q], q.name))
+        for f in self.inputs + self.outputs:
+            call_fill.append("A.b_%s = %s;" % (self.fn(f), f.name))
+        w.open('extern "C" int pipeline_%s_dev(%s, void* stream)' % (name,
+                                                                    sig))
+        w("pm_args A; memset(&A, 0, sizeof(A));")
+        for line in call_fill:
+            w(line)
+        w("pm_status = pm_run(A, (cudaStream_t)stream);")
+        w("return pm_status;")
+        w.close()
+        w("")
+        # ---- graph replay ----
+        w("static cudaGraphExec_t pm_graph_exec = nullptr;")
+        w("static pm_args pm_graph_key;")
+        w("static void* pm_graph_ws = nullptr;")
+        w("static cudaStream_t pm_graph_stream = nullptr;")
+        w("// Replays a CUDA graph of the whole pipeline; the graph is")
+        w("// (re)captured when the arguments or the workspace change.")
+        w.open('extern "C" int pipeline_%s_graph(%s, void* stream)' % (name,
+                                                                      sig))
+        w("pm_args A; memset(&A, 0, sizeof(A));")
+        for line in call_fill:
+            w(line)
+        w("int dev = 0; cudaGetDevice(&dev);")
+        w("void* wsnow = (dev >= 0 && dev < 64) ? pm_ws_arena.ptr[dev] : "
+          "nullptr;")
+        w.open("if (!pm_graph_exec || wsnow != pm_graph_ws || memcmp(&A, "
+               "&pm_graph_key, sizeof(A)) != 0)")
+        w("pm_args B = A;")
+        w("int st = pm_run(B, (cudaStream_t)stream);  // sizes workspace, "
+          "uploads tables")
+        w("if (st) return pm_status = st;")
+        w("if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) "
+          "return pm_status = PM_ERR_CUDA;")
+        w("if (!pm_graph_stream && cudaStreamCreateWithFlags(&pm_graph_stream,"
+          " cudaStreamNonBlocking) != cudaSuccess) return pm_status = "
+          "PM_ERR_CUDA;")
+        w("if (pm_graph_exec) { cudaGraphExecDestroy(pm_graph_exec); "
+          "pm_graph_exec = nullptr; }")
+        w("cudaGraph_t g = nullptr;")
+        w("if (cudaStreamBeginCapture(pm_graph_stream, "
+          "cudaStreamCaptureModeThreadLocal) != cudaSuccess) return "
+          "pm_status = PM_ERR_CUDA;")
+        w("pm_args Cc = A;")
+        w("st = pm_run(Cc, pm_graph_stream);")
+        w("cudaError_t e = cudaStreamEndCapture(pm_graph_stream, &g);")
+        w("if (st || e != cudaSuccess) { if (g) cudaGraphDestroy(g); "
+          "cudaGetLastError(); return pm_status = st ? st : PM_ERR_CUDA; }")
+        w("e = cudaGraphInstantiate(&pm_graph_exec, g, 0);")
+        w("cudaGraphDestroy(g);")
+        w("if (e != cudaSuccess) { pm_graph_exec = nullptr; return "
+          "pm_status = PM_ERR_CUDA; }")
+        w("pm_graph_key = A;")
+        w("pm_graph_ws = pm_ws_arena.ptr[dev];")
+        w.close()
+        w("if (cudaGraphLaunch(pm_graph_exec, (cudaStream_t)stream) != "
+          "cudaSuccess) return pm_status = PM_ERR_CUDA;")
+        w("return pm_status = PM_OK;")
+        w.close()
+        w("")
+        # ---- host pointers (the reference's ABI) ----
+        self.gen_host_entry(sig, call_fill)
+        # ---- batch ----
+        self.gen_batch_entry()
+        # ---- status ----
+        w('extern "C" int pipeline_%s_status(void) { return pm_status; }'
+          % name)
+        w.open('extern "C" int pipeline_%s_check(void)' % name)
+        w("unsigned v = 0;")
+        w("if (cudaDeviceSynchronize() != cudaSuccess) return PM_ERR_CUDA;")
+        w("if (cudaMemcpyFromSymbol(&v, pm_err_word, sizeof(v)) != "
+          "cudaSuccess) return PM_ERR_CUDA;")
+        w("return v ? PM_ERR_KERNEL : PM_OK;")
+        w.close()
+        w('extern "C" void pipeline_%s_clear_error(void) { unsigned z = 0; '
+          'cudaMemcpyToSymbol(pm_err_word, &z, sizeof(z)); pm_status = 0; }'
+          % name)
+        w("")
+
+    def gen_host_entry(self, sig, call_fill):
+        w = self.w
+        name = self.pname
+        ctx = ExprCtx(w, 'device', self.pmap, None)
+        nin, nout = len(self.inputs), len(self.outputs)
+        w("static pm_arena pm_host_in[%d];" % max(nin, 1))
+        w("static pm_arena pm_host_out[%d];" % max(nout, 1))
+        w("static cudaStream_t pm_host_stream[64];")
+        w.open('extern "C" void pipeline_%s(%s)' % (name, sig))
+        w("pm_args A; memset(&A, 0, sizeof(A));")
+        for line in call_fill:
+            w(line)
+        w("int dev = 0; cudaGetDevice(&dev);")
+        w("if (dev < 0 || dev >= 64) { pm_status = PM_ERR_CUDA; return; }")
+        w("if (!pm_host_stream[dev] && cudaStreamCreateWithFlags("
+          "&pm_host_stream[dev], cudaStreamNonBlocking) != cudaSuccess) "
+          "{ pm_status = PM_ERR_CUDA; return; }")
+        w("cudaStream_t s = pm_host_stream[dev];")
+        self.declare_params(w, "A")
+        w("int st = pm_validate(A);")
+        w("if (st) { pm_status = st; return; }")
+        for i, f in enumerate(self.inputs + self.outputs):
+            n = self.fn(f)
+            arena = "pm_host_in[%d]" % i if i < nin else \
+                "pm_host_out[%d]" % (i - nin)
+            ext = " * ".join("(size_t)pm_nonneg((%s) - (%s) + 1)" % (hi, lo)
+                             for lo, hi in self.dom_exprs(f, ctx))
+            w("const size_t nb_%s = (size_t)%d * %s;" % (n, f.typ.size(), ext))
+            w("void* dv_%s = nullptr;" % n)
+            w("if (pm_arena_get(&%s, nb_%s, &dv_%s)) { pm_status = "
+              "PM_ERR_CUDA; return; }" % (arena, n, n))
+        for f in self.inputs:
+            n = self.fn(f)
+            w("if (nb_%s && cudaMemcpyAsync(dv_%s, %s, nb_%s, "
+              "cudaMemcpyHostToDevice, s) != cudaSuccess) { pm_status = "
+              "PM_ERR_CUDA; return; }" % (n, n, f.name, n))
+        for f in self.outputs:
+            n = self.fn(f)
+            box = self.written_box(f)
+            if box is None:
+                # coverage is not a box: keep the caller's untouched points
+                w("if (nb_%s && cudaMemcpyAsync(dv_%s, %s, nb_%s, "
+                  "cudaMemcpyHostToDevice, s) != cudaSuccess) { pm_status = "
+                  "PM_ERR_CUDA; return; }" % (n, n, f.name, n))
+        for f in self.inputs + self.outputs:
+            n = self.fn(f)
+            w("A.b_%s = dv_%s;" % (n, n))
+        w("st = pm_run(A, s);")
+        w("if (st) { pm_status = st; cudaStreamSynchronize(s); return; }")
+        for f in self.outputs:
+            self.gen_d2h(f, ctx)
+        w("if (cudaStreamSynchronize(s) != cudaSuccess) { pm_status = "
+          "PM_ERR_CUDA; return; }")
+        w("unsigned kerr = 0;")
+        w("cudaMemcpyFromSymbol(&kerr, pm_err_word, sizeof(kerr));")
+        w("pm_status = kerr ? PM_ERR_KERNEL : PM_OK;")
+        w.close()
+        w("")
+
+    def written_box(self, f):
+        """Per-dim (lo, hi) expressions of the points of output ``f`` that
+        the pipeline writes, when they form a box; None otherwise."""
+        parts = part_boxes(f)
+        if not parts or any(not b.exact for b, _, _, _ in parts):
+            return None
+        env = self.p.int_env()
+        try:
+            vals = [b.evaluate(env) for b, _, _, _ in parts]
+        except Exception:
+            return None
+        vs = f.variables
+        if len(parts) > 1:
+            # union is a box when all parts agree except on one dim where
+            # their intervals are disjoint and contiguous
+            diff = [v for v in vs if len(set(val[v] for val in vals)) > 1]
+            if len(diff) > 1:
+                return None
+            if diff:
+                v = diff[0]
+                iv = sorted(val[v] for val in vals)
+                for (a0, a1), (b0, b1) in zip(iv, iv[1:]):
+                    if b0 != a1 + 1:
+                        return None
+        out = []
+        for d, v in enumerate(vs):
+            los, his = [], []
+            for b, _, _, _ in parts:
+                lo = b.lo[v][0]
+                for e in b.lo[v][1:]:
+                    lo = C.Max(lo, e, typeCheck=False)
+                hi = b.hi[v][0]
+                for e in b.hi[v][1:]:
+                    hi = C.Min(hi, e, typeCheck=False)
+                los.append(lo)
+                his.append(hi)
+            lo = los[0]
+            for e in los[1:]:
+                lo = C.Min(lo, e, typeCheck=False)
+            hi = his[0]
+            for e in his[1:]:
+                hi = C.Max(hi, e, typeCheck=False)
+            out.append((lo, hi))
+        return out
+
+    def gen_d2h(self, f, ctx):
+        w = self.w
+        n = self.fn(f)
+        box = self.written_box(f)
+        es = f.typ.size()
+        if box is None:
+            w("if (nb_%s && cudaMemcpyAsync(%s, dv_%s, nb_%s, "
+              "cudaMemcpyDeviceToHost, s) != cudaSuccess) { pm_status = "
+              "PM_ERR_CUDA; return; }" % (n, f.name, n, n))
+            return
+        nd = len(f.domain)
+        w.open("")
+        for d, dom in enumerate(f.domain):
+            w("const long long D%d_lo = %s, D%d_hi = %s;" % (
+                d, ctx.expr(dom.lowerBound, {}), d,
+                ctx.expr(dom.upperBound, {})))
+            w("const long long B%d_lo = pm_llmax(D%d_lo, %s), B%d_hi = "
+              "pm_llmin(D%d_hi, %s);" % (d, d, ctx.expr(box[d][0], {}), d, d,
+                                         ctx.expr(box[d][1], {})))
+        w("bool nonempty = %s;" % " && ".join(
+            "B%d_lo <= B%d_hi" % (d, d) for d in range(nd)))
+        w("long long S%d = 1;" % (nd - 1))
+        for d in range(nd - 2, -1, -1):
+            w("long long S%d = S%d * (D%d_hi - D%d_lo + 1);" % (d, d + 1,
+                                                                d + 1, d + 1))
+        w.open("if (nonempty)")
+        if nd == 1:
+            w("size_t o = (size_t)(B0_lo - D0_lo) * %d;" % es)
+            w("if (cudaMemcpyAsync((char*)%s + o, (char*)dv_%s + o, "
+              "(size_t)(B0_hi - B0_lo + 1) * %d, cudaMemcpyDeviceToHost, s) "
+              "!= cudaSuccess) { pm_status = PM_ERR_CUDA; return; }" % (
+                  f.name, n, es))
+        else:
+            # loops over the outer dims, one 2-D copy per outer point
+            for d in range(nd - 2):
+                w.open("for (long long i%d = B%d_lo; i%d <= B%d_hi; ++i%d)" % (
+                    d, d, d, d, d))
+            outer = " + ".join(["(i%d - D%d_lo) * S%d" % (d, d, d)
+                                for d in range(nd - 2)] or ["0"])
+            a, b = nd - 2, nd - 1
+            w("size_t o = (size_t)((%s) + (B%d_lo - D%d_lo) * S%d + (B%d_lo - "
+              "D%d_lo)) * %d;" % (outer, a, a, a, b, b, es))
+            w("size_t pitch = (size_t)S%d * %d;" % (a, es))
+            w("if (cudaMemcpy2DAsync((char*)%s + o, pitch, (char*)dv_%s + o, "
+              "pitch, (size_t)(B%d_hi - B%d_lo + 1) * %d, (size_t)(B%d_hi - "
+              "B%d_lo + 1), cudaMemcpyDeviceToHost, s) != cudaSuccess) "
+              "{ pm_status = PM_ERR_CUDA; return; }" % (f.name, n, b, b, es,
+                                                         a, a))
+            for d in range(nd - 2):
+                w.close()
+        w.close()
+        w.close()
+
+    def gen_batch_entry(self):
+        w = self.w
+        name = self.pname
+        nin, nout = len(self.inputs), len(self.outputs)
+        w("static pm_arena pm_batch_arena;")
+        w("static char* pm_batch_pinned = nullptr;")
+        w("static size_t pm_batch_pinned_cap = 0;")
+        w("// Batched execution: n images (each with its own parameters) run")
+        w("// through each group in one launch; a CTA maps its block index to")
+        w("// (image, tile) through the per-image tile prefix.")
+        w.open('extern "C" int pipeline_%s_batch(int n, const int* iparams, '
+               'const float* fparams, void* const* inputs, void* const* '
+               'outputs, void* stream)' % name)
+        w("cudaStream_t s = (cudaStream_t)stream;")
+        w("if (n <= 0) return pm_status = PM_OK;")
+        w("std::vector<pm_args> As(n);")
+        w("std::vector<size_t> wsoffs((size_t)n * %d);" % max(self.nslots, 1))
+        w("size_t total = 0;")
+        w.open("for (int i = 0; i < n; ++i)")
+        w("pm_args& A = As[i]; memset(&A, 0, sizeof(A));")
+        for j, q in enumerate(self.iparams):
+            w("A.%s = iparams[(size_t)i * %d + %d];" % (
+                self.pmap[q], len(self.iparams), j))
+        for j, q in enumerate(self.fparams):
+            w("A.%s = fparams[(size_t)i * %d + %d];" % (
+                self.pmap[q], len(self.fparams), j))
+        for j, f in enumerate(self.inputs):
+            w("A.b_%s = inputs[(size_t)i * %d + %d];" % (self.fn(f), nin, j))
+        for j, f in enumerate(self.outputs):
+            w("A.b_%s = outputs[(size_t)i * %d + %d];" % (self.fn(f), nout,
+                                                          j))
+        w("int st = pm_validate(A); if (st) return pm_status = st;")
+        w("size_t t = 0; pm_ws_layout(A, &wsoffs[(size_t)i * %d], &t);" %
+          max(self.nslots, 1))
+        w("for (int k = 0; k < %d; ++k) wsoffs[(size_t)i * %d + k] += total;"
+          % (self.nslots, max(self.nslots, 1)))
+        w("total += pm_align256(t);")
+        w.close()
+        w("size_t descs_bytes = pm_batch_desc_bytes(n);")
+        w("void* ws = nullptr;")
+        w("if (pm_arena_get(&pm_batch_arena, total + descs_bytes, &ws)) "
+          "return pm_status = PM_ERR_CUDA;")
+        w("for (int i = 0; i < n; ++i) As[i].ws = (char*)ws;")
+        w("char* ddesc = (char*)ws + total;")
+        w("if (!pm_batch_event && cudaEventCreateWithFlags(&pm_batch_event, "
+          "cudaEventDisableTiming) != cudaSuccess) return pm_status = "
+          "PM_ERR_CUDA;")
+        w("cudaEventSynchronize(pm_batch_event);  // previous upload done")
+        w.open("if (pm_batch_pinned_cap < descs_bytes)")
+        w("if (pm_batch_pinned) cudaFreeHost(pm_batch_pinned);")
+        w("pm_batch_pinned = nullptr; pm_batch_pinned_cap = 0;")
+        w("if (cudaMallocHost((void**)&pm_batch_pinned, descs_bytes) != "
+          "cudaSuccess) return pm_status = PM_ERR_CUDA;")
+        w("pm_batch_pinned_cap = descs_bytes;")
+        w.close()
+        w("size_t doff = 0; int st = 0;")
+        for fnm in self.batch_fns:
+            w("if ((st = %s(As.data(), wsoffs.data(), %d, n, pm_batch_pinned, "
+              "ddesc, &doff, s))) return pm_status = st;" % (
+                  fnm, max(self.nslots, 1)))
+        w("return pm_status = PM_OK;")
+        w.close()
+        w("")
+
+    def gen_header(self):
+        name = self.pname
+        sig = ", ".join(self.abi_params())
+        lines = [
+            "/* pipeline_%s -- C ABI of the PolyMage pipeline '%s' built for "
+            "NVIDIA B200 (sm_100a)." % (name, self.p.name),
+            " * Generated by polymage_b200; argument order: parameters, then "
+            "inputs, then",
+            " * outputs, each sorted by name (the reference's generated "
+            "pipeline_<name> ABI). */",
+            "#pragma once",
+            "#ifdef __cplusplus",
+            'extern "C" {',
+            "#endif",
+            "/* host buffers, synchronous (reference ABI) */",
+            "void pipeline_%s(%s);" % (name, sig),
+            "/* device buffers, asynchronous on `stream` (cudaStream_t); "
+            "returns a PM status */",
+            "int pipeline_%s_dev(%s, void* stream);" % (name, sig),
+            "/* same as _dev through a CUDA graph captured on first use */",
+            "int pipeline_%s_graph(%s, void* stream);" % (name, sig),
+            "/* n images; iparams: n x %d int params, fparams: n x %d float "
+            "params, each row in" % (len(self.iparams), len(self.fparams)),
+            " * name order; inputs: n x %d device pointers, outputs: n x %d "
+            "device pointers */" % (len(self.inputs), len(self.outputs)),
+            "int pipeline_%s_batch(int n, const int* iparams, const float* "
+            "fparams, void* const* inputs, void* const* outputs, void* "
+            "stream);" % name,
+            "/* status of the last call: 0 ok, 1 bad parameters, 2 CUDA "
+            "error, 3 kernel error */",
+            "int pipeline_%s_status(void);" % name,
+            "/* synchronizes and reports the device error word */",
+            "int pipeline_%s_check(void);" % name,
+            "void pipeline_%s_clear_error(void);" % name,
+            "#ifdef __cplusplus",
+            "}",
+            "#endif",
+        ]
+        return "\n".join(lines) + "\n"
+
+
+# ---------------------------------------------------------------------------
+class StencilGen(object):
+    """Kernel + launcher of one fused stencil group."""
+
+    def __init__(self, pg, group):
+        self.pg = pg
+        self.g = group
+        self.plan = group.plan
+        self.k = "pm_%s_g%d" % (pg.pname, group.level_time)
+
+    def node_name(self, n):
+        return self.pg.fn(n.func)
+
+    def generate(self):
+        pg = self.pg
+        plan = self.plan
+        w = pg.w
+        k = self.k
+        anchor = plan.anchor
+        na = anchor.ndims
+        stage_nodes = [n for n in plan.nodes if n.role == 'stage']
+        glob_ext = [x for x in plan.externals
+                    if plan.ext_role[x] == 'global']
+        outs = [n for n in plan.nodes if n.role == 'out']
+        self.outs = outs
+        self.stage_nodes = stage_nodes
+        # buffers the kernel touches
+        bufs = []
+        for n in stage_nodes:
+            bufs.append(n.func)
+        for x in glob_ext:
+            bufs.append(x)
+        for n in outs:
+            bufs.append(n.func)
+        self.bufs = bufs
+        pg.meta['groups'].append({
+            'kernel': k, 'kind': 'stencil', 'threads': plan.threads,
+            'smem': plan.smem_bytes, 'tile': plan.tile,
+            'stages': [f.name for f in plan.funcs],
+            'materialized': [f.name for f in plan.steps],
+            'staged': [n.name for n in stage_nodes],
+            'features': plan.features()})
+        # ---- descriptor -------------------------------------------------------
+        w("// ---- group %d: %s (anchor %s, tile %s, %d threads, %d B smem)"
+          % (self.g.level_time, ", ".join(f.name for f in plan.funcs),
+             anchor.name, plan.tile, plan.threads, plan.smem_bytes))
+        w.open("struct __align__(64) %s_desc" % k)
+        for n in stage_nodes:
+            w("CUtensorMap tm_%s;" % self.node_name(n))
+        for prm in pg.params:
+            w("%s %s;" % (pg.ptype(prm), pg.pmap[prm]))
+        for f in bufs:
+            w("%s%s* b_%s;" % ("" if any(f is n.func for n in outs)
+                               else "const ", ctype(f.typ), pg.fn(f)))
+        w("int glo[%d], ghi[%d], gn[%d];" % (na, na, na))
+        w("int tile_base;")
+        for n in stage_nodes:
+            w("int tma_%s;" % self.node_name(n))
+        w.close("};")
+        w.open("struct %s_launch" % k)
+        w("%s_desc d0;" % k)
+        w("const %s_desc* descs;" % k)
+        w("int nimg;")
+        w.close("};")
+        w("")
+        self.gen_kernel()
+        self.gen_launcher()
+
+    # ---- kernel -------------------------------------------------------------
+    def gen_kernel(self):
+        pg = self.pg
+        plan = self.plan
+        w = pg.w
+        k = self.k
+        anchor = plan.anchor
+        na = anchor.ndims
+        nt = plan.threads
+        w('extern "C" __global__ void __launch_bounds__(%d) %s(const '
+          '__grid_constant__ %s_launch L)' % (nt, k, k))
+        w.open("")
+        w("extern __shared__ __align__(128) unsigned char pm_smem[];")
+        w("const int tile = blockIdx.x;")
+        w("const %s_desc* Dp = &L.d0;" % k)
+        w("if (L.nimg > 1) Dp = L.descs + pm_find_image(L.descs, L.nimg, "
+          "tile);")
+        w("const %s_desc& D = *Dp;" % k)
+        pg.declare_params(w, "D")
+        ctx = ExprCtx(w, 'device', pg.pmap, self.reader)
+        self.ctx = ctx
+        # tile coordinates
+        w("int rem = tile - D.tile_base;")
+        for d in range(na - 1, 0, -1):
+            w("const int t%d = rem %% D.gn[%d]; rem /= D.gn[%d];" % (d, d, d))
+        w("const int t0 = rem;")
+        for d in range(na):
+            w("const int a_lo%d = D.glo[%d] + t%d * %d;" % (d, d, d,
+                                                           plan.tile[d]))
+            w("const int a_hi%d = pm_imin(a_lo%d + %d, D.ghi[%d]);" % (
+                d, d, plan.tile[d] - 1, d))
+        # domains and strides of everything we touch
+        need_stride = set(id(f) for f in self.bufs)
+        for n in plan.nodes:
+            pg.declare_domain(w, n.func, ctx, id(n.func) in need_stride)
+        for f in self.bufs:
+            if f not in plan.node_of:
+                pg.declare_domain(w, f, ctx, True)
+        # region inference
+        self.gen_regions()
+        # buffers
+        for f in self.bufs:
+            w("%s%s* __restrict__ b_%s = D.b_%s;" % (
+                "" if any(f is n.func for n in self.outs) else "const ",
+                ctype(f.typ), pg.fn(f), pg.fn(f)))
+        for n in plan.nodes:
+            if n.in_smem:
+                nm = self.node_name(n)
+                w("%s* sm_%s = reinterpret_cast<%s*>(pm_smem + %d);" % (
+                    ctype(n.func.typ), nm, ctype(n.func.typ), n.smem_off))
+                self.decl_smem_origin(n)
+        self.gen_staging()
+        for f in plan.steps:
+            self.gen_step(f)
+        w.close()
+        w("")
+
+    def empty_expr(self, n):
+        nm = self.node_name(n)
+        return " || ".join("r_%s_lo%d > r_%s_hi%d" % (nm, d, nm, d)
+                           for d in range(n.ndims))
+
+    def gen_regions(self):
+        pg = self.pg
+        plan = self.plan
+        w = pg.w
+        ctx = self.ctx
+        na = plan.anchor.ndims
+        big = "0x3fffffff"
+        for n in plan.nodes:
+            nm = self.node_name(n)
+            fnm = pg.fn(n.func)
+            nd = n.ndims
+            if n.func is plan.anchor:
+                for d in range(nd):
+                    w("const int r_%s_lo%d = pm_imax(a_lo%d, d_%s_lo%d), "
+                      "r_%s_hi%d = pm_imin(a_hi%d, d_%s_hi%d);" % (
+                          nm, d, d, fnm, d, nm, d, d, fnm, d))
+                continue
+            if n.role == 'out':
+                owner = " && ".join("t%d == 0" % kk
+                                    for kk in range(na - nd)) or "true"
+                for d in range(nd):
+                    kk = n.owned_map[d]
+                    w("int o_%s_lo%d = (%s) ? pm_imax(a_lo%d, d_%s_lo%d) : "
+                      "%s;" % (nm, d, owner, kk, fnm, d, big))
+                    w("int o_%s_hi%d = (%s) ? pm_imin(a_hi%d, d_%s_hi%d) : "
+                      "-%s;" % (nm, d, owner, kk, fnm, d, big))
+                    w("int r_%s_lo%d = o_%s_lo%d, r_%s_hi%d = o_%s_hi%d;" % (
+                        nm, d, nm, d, nm, d, nm, d))
+            else:
+                for d in range(nd):
+                    w("int r_%s_lo%d = %s, r_%s_hi%d = -%s;" % (nm, d, big,
+                                                                nm, d, big))
+            for m, fns in n.uses:
+                mn = self.node_name(m)
+                w.open("if (!(%s))" % self.empty_expr(m))
+                for d, fn in enumerate(fns):
+                    if fn.kind == 'mono':
+                        a = ctx.expr(fn.expr, {fn.var: "r_%s_lo%d" % (
+                            mn, fn.cdim)})
+                        b = ctx.expr(fn.expr, {fn.var: "r_%s_hi%d" % (
+                            mn, fn.cdim)})
+                    elif fn.kind == 'const':
+                        a = b = ctx.expr(fn.expr, {})
+                    else:
+                        a, b = "d_%s_lo%d" % (fnm, d), "d_%s_hi%d" % (fnm, d)
+                    w("{ const int ea = %s, eb = %s; r_%s_lo%d = pm_imin("
+                      "r_%s_lo%d, pm_imin(ea, eb)); r_%s_hi%d = pm_imax("
+                      "r_%s_hi%d, pm_imax(ea, eb)); }" % (
+                          a, b, nm, d, nm, d, nm, d, nm, d))
+                w.close()
+            for d in range(nd):
+                w("r_%s_lo%d = pm_imax(r_%s_lo%d, d_%s_lo%d); r_%s_hi%d = "
+                  "pm_imin(r_%s_hi%d, d_%s_hi%d);" % (nm, d, nm, d, fnm, d,
+                                                      nm, d, nm, d, fnm, d))
+
+    def decl_smem_origin(self, n):
+        """Smem layout of a node: dense [E0][E1]..[E_inner] (inner padded
+        for staged inputs); sb_<n> is the linear offset of the origin."""
+        w = self.pg.w
+        nm = self.node_name(n)
+        fnm = self.pg.fn(n.func)
+        ext = list(n.ext)
+        if n.role == 'stage':
+            es = n.func.typ.size()
+            al = max(1, 16 // es)
+            ext[-1] = n.pad_inner
+            nd = n.ndims
+            w("const int so_%s_%d = (r_%s_lo%d - d_%s_lo%d) & ~%d;" % (
+                nm, nd - 1, nm, nd - 1, fnm, nd - 1, al - 1))
+            org = ["r_%s_lo%d" % (nm, d) for d in range(nd - 1)] + \
+                ["(d_%s_lo%d + so_%s_%d)" % (fnm, nd - 1, nm, nd - 1)]
+        else:
+            org = ["r_%s_lo%d" % (nm, d) for d in range(n.ndims)]
+        strides = []
+        s = 1
+        for e in reversed(ext):
+            strides.insert(0, s)
+            s *= e
+        n._sm_strides = strides
+        n._sm_ext = ext
+        terms = ["%s * %d" % (o, st) for o, st in zip(org, strides)]
+        w("const int sb_%s = %s;" % (nm, " + ".join(terms)))
+        for d in range(n.ndims):
+            w("(void)r_%s_hi%d;" % (nm, d))
+
+    def smem_index(self, n, args):
+        ctx = self.ctx
+        nm = self.node_name(n)
+        fnm = self.pg.fn(n.func)
+        terms = []
+        for d, (a, st) in enumerate(zip(args, n._sm_strides)):
+            s = ctx.index(a)
+            if is_data_dependent(a):
+                if n.role == 'stage':
+                    s = "pm_clampi(%s, d_%s_lo%d, d_%s_hi%d)" % (s, fnm, d,
+                                                                fnm, d)
+                else:
+                    s = "pm_clampi(%s, r_%s_lo%d, r_%s_hi%d)" % (s, nm, d,
+                                                                nm, d)
+            terms.append(s if st == 1 else "%s * %d" % (s, st))
+        return "%s - sb_%s" % (" + ".join(terms), nm)
+
+    # ---- producer reads ------------------------------------------------------
+    def reader(self, f, args, ctx):
+        pg = self.pg
+        plan = self.plan
+        key = (pg.fn(f), tuple(ctx.index(a) if not is_data_dependent(a)
+                                else ctx.expr(a, {}) for a in args))
+        hit = ctx.lookup(key)
+        if hit is not None:
+            return hit
+        w = pg.w
+        node = plan.node_of.get(f)
+        t = ctx.temp()
+        if node is not None and node.in_smem:
+            w("const %s %s = sm_%s[%s];" % (ctype(f.typ), t,
+                                            self.node_name(node),
+                                            self.smem_index(node, args)))
+        elif f in plan.role and plan.role[f] == 'inline':
+            self.emit_inline(f, args, t)
+        elif f in plan.role:
+            raise CodegenError("internal: %s read but not available" %
+                               f.name)
+        else:
+            w("const %s %s = __ldg(b_%s + (%s));" % (
+                ctype(f.typ), t, pg.fn(f), pg.gindex(f, args, ctx)))
+        ctx.define(key, t)
+        return t
+
+    def emit_inline(self, f, args, t):
+        """Compute an inlined stage's value at ``args`` into temp ``t``."""
+        w = self.pg.w
+        ctx = self.ctx
+        w("%s %s = 0;" % (ctype(f.typ), t))
+        bind = dict(zip(f.variables, args))
+        self.emit_cases(f, bind, t, None)
+
+    def emit_cases(self, f, bind, target, written_flag):
+        """Evaluate ``f``'s definition at the bound point into ``target``
+        (already 0); later cases take precedence, as in the reference
+        where later parts' loops overwrite earlier ones."""
+        w = self.pg.w
+        ctx = self.ctx
+        parts = body_parts(f)
+        if len(parts) == 1 and parts[0][0] is None:
+            e = ctx.expr(parts[0][1], bind)
+            w("%s = (%s)(%s);" % (target, ctype(f.typ), e))
+            if written_flag:
+                w("%s = true;" % written_flag)
+            return
+        first = True
+        for cond, expr, red in reversed(parts):
+            ctx.push()
+            c = ctx.cond(cond, bind) if cond is not None else "true"
+            w.open("%sif (%s)" % ("" if first else "else ", c))
+            e = ctx.expr(expr, bind)
+            w("%s = (%s)(%s);" % (target, ctype(f.typ), e))
+            if written_flag:
+                w("%s = true;" % written_flag)
+            w.close()
+            ctx.pop()
+            first = False
+
+    # ---- staging of external producers ------------------------------------------
+    def gen_staging(self):
+        pg = self.pg
+        plan = self.plan
+        w = pg.w
+        stage_nodes = self.stage_nodes
+        if not stage_nodes:
+            return
+        bar_off = plan.smem_bytes - 128
+        w("uint64_t* pm_bar = reinterpret_cast<uint64_t*>(pm_smem + %d);" %
+          bar_off)
+        conds = []
+        for n in stage_nodes:
+            nm = self.node_name(n)
+            w("const bool use_tma_%s = D.tma_%s && !(%s);" % (
+                nm, nm, self.empty_expr(n)))
+            conds.append("use_tma_%s" % nm)
+        w("const bool any_tma = %s;" % " || ".join(conds))
+        w.open("if (any_tma && threadIdx.x == 0)")
+        w("pm_mbar_init(pm_bar, 1);")
+        w("pm_fence_barrier_init();")
+        w.close()
+        w("__syncthreads();")
+        w.open("if (any_tma && threadIdx.x == 0)")
+        w("uint32_t bytes = 0;")
+        for n in stage_nodes:
+            nm = self.node_name(n)
+            box = 1
+            for e in n._sm_ext:
+                box *= e
+            w("if (use_tma_%s) bytes += %du;" % (nm, box * n.func.typ.size()))
+        w("pm_mbar_arrive_expect_tx(pm_bar, bytes);")
+        for n in stage_nodes:
+            nm = self.node_name(n)
+            fnm = pg.fn(n.func)
+            nd = n.ndims
+            coords = ["so_%s_%d" % (nm, nd - 1)]
+            for d in range(nd - 2, -1, -1):
+                coords.append("r_%s_lo%d - d_%s_lo%d" % (nm, d, fnm, d))
+            w("if (use_tma_%s) pm_tma_load_%dd(sm_%s, &D.tm_%s, pm_bar, %s);"
+              % (nm, nd, nm, nm, ", ".join(coords)))
+        w.close()
+        # cooperative fallback
+        for n in stage_nodes:
+            nm = self.node_name(n)
+            fnm = pg.fn(n.func)
+            nd = n.ndims
+            ext = n._sm_ext
+            tot = 1
+            for e in ext:
+                tot *= e
+            w.open("if (!D.tma_%s && !(%s))" % (nm, self.empty_expr(n)))
+            w.open("for (int i = threadIdx.x; i < %d; i += %d)" % (
+                tot, plan.threads))
+            self.decompose("i", ext, "j")
+            inb = []
+            coords = []
+            for d in range(nd):
+                if d == nd - 1:
+                    c = "so_%s_%d + j%d" % (nm, d, d)
+                else:
+                    c = "r_%s_lo%d - d_%s_lo%d + j%d" % (nm, d, fnm, d, d)
+                w("const int c%d = %s;" % (d, c))
+                inb.append("c%d >= 0 && c%d <= d_%s_hi%d - d_%s_lo%d" % (
+                    d, d, fnm, d, fnm, d))
+                coords.append("(long long)c%d * s_%s_%d" % (d, fnm, d))
+            w("sm_%s[i] = (%s) ? __ldg(b_%s + (%s)) : (%s)0;" % (
+                nm, " && ".join(inb), fnm, " + ".join(coords),
+                ctype(n.func.typ)))
+            w.close()
+            w.close()
+        w.open("if (any_tma)")
+        w("pm_mbar_wait(pm_bar, 0, &pm_err_word);")
+        w.close()
+        w("__syncthreads();")
+
+    def decompose(self, iv, ext, prefix):
+        w = self.pg.w
+        nd = len(ext)
+        if nd == 1:
+            w("const int %s0 = %s;" % (prefix, iv))
+            return
+        w("int rr = %s;" % iv)
+        for d in range(nd - 1, 0, -1):
+            w("const int %s%d = rr %% %d; rr /= %d;" % (prefix, d, ext[d],
+                                                       ext[d]))
+        w("const int %s0 = rr;" % prefix)
+
+    # ---- materialized stages -------------------------------------------------
+    def gen_step(self, f):
+        pg = self.pg
+        plan = self.plan
+        w = pg.w
+        n = plan.node_of[f]
+        nm = self.node_name(n)
+        fnm = pg.fn(f)
+        nd = n.ndims
+        comp = pg.p.func_map[f]
+        is_out = n.role == 'out'
+        pipe_out = comp.is_output
+        ext = n.ext if n.in_smem else \
+            [min(e, t) for e, t in zip(n.ext, plan.tile[plan.anchor.ndims -
+                                                        nd:])]
+        tot = 1
+        for e in ext:
+            tot *= e
+        w("// stage %s (%s%s)" % (f.name, n.role,
+                                  "+smem" if n.also_smem else ""))
+        w.open("")
+        w.open("for (int i = threadIdx.x; i < %d; i += %d)" % (
+            tot, plan.threads))
+        self.decompose("i", ext, "j")
+        lv = _loop_vars(nd)
+        for d in range(nd):
+            w("const int q%d = r_%s_lo%d + j%d;" % (d, nm, d, d))
+        w("if (%s) continue;" % " || ".join("q%d > r_%s_hi%d" % (d, nm, d)
+                                           for d in range(nd)))
+        ctx = self.ctx
+        ctx.push()
+        bind = dict(zip(f.variables, lv))
+        w("%s v = 0;" % ctype(f.typ))
+        flag = None
+        if is_out and pipe_out:
+            w("bool wr = false;")
+            flag = "wr"
+        self.emit_cases(f, bind, "v", flag)
+        if n.in_smem:
+            w("sm_%s[i] = v;" % nm)
+        if is_out:
+            own = ""
+            if n.func is not plan.anchor and n.also_smem:
+                own = " && ".join("q%d >= o_%s_lo%d && q%d <= o_%s_hi%d" % (
+                    d, nm, d, d, nm, d) for d in range(nd))
+            cond = " && ".join(x for x in [own, flag or ""] if x)
+            idx = " + ".join(
+                ["(long long)(q%d - d_%s_lo%d) * s_%s_%d" % (d, fnm, d, fnm, d)
+                 for d in range(nd)])
+            if cond:
+                w("if (%s) b_%s[%s] = v;" % (cond, fnm, idx))
+            else:
+                w("b_%s[%s] = v;" % (fnm, idx))
+        ctx.pop()
+        w.close()
+        w.close()
+        if n.in_smem:
+            w("__syncthreads();")
+
+    # ---- launcher -------------------------------------------------------------
+    def gen_launcher(self):
+        pg = self.pg
+        plan = self.plan
+        w = pg.w
+        k = self.k
+        anchor = plan.anchor
+        na = anchor.ndims
+        ctx = ExprCtx(w, 'device', pg.pmap, None)
+        fill = "fill_" + k
+        # descriptor filler shared by the single and batched launches
+        w.open("static int %s(%s_desc& D, const pm_args& A, const size_t* "
+               "wsoff, long long* ntiles)" % (fill, k))
+        pg.declare_params(w, "A")
+        for prm in pg.params:
+            w("D.%s = %s;" % (pg.pmap[prm], pg.pmap[prm]))
+        for f in self.bufs:
+            w("D.b_%s = (%s%s*)(%s);" % (
+                pg.fn(f), "" if any(f is n.func for n in self.outs)
+                else "const ", ctype(f.typ), pg.buf_expr(f)))
+        # grid: union of the out nodes' domains along the anchor dims
+        for kk in range(na):
+            w("long long glo%d = 0x3fffffff, ghi%d = -0x3fffffff;" % (kk, kk))
+        for n in self.outs:
+            for d, dom in enumerate(n.func.domain):
+                kk = n.owned_map[d] if n.func is not anchor else d
+                w("glo%d = pm_llmin(glo%d, %s); ghi%d = pm_llmax(ghi%d, %s);"
+                  % (kk, kk, ctx.expr(dom.lowerBound, {}), kk, kk,
+                     ctx.expr(dom.upperBound, {})))
+        w("long long tot = 1;")
+        for kk in range(na):
+            w("if (ghi%d < glo%d) { *ntiles = 0; return PM_OK; }" % (kk, kk))
+            w("D.glo[%d] = (int)glo%d; D.ghi[%d] = (int)ghi%d;" % (kk, kk, kk,
+                                                                  kk))
+            w("D.gn[%d] = (int)((ghi%d - glo%d + %d) / %d);" % (
+                kk, kk, kk, plan.tile[kk], plan.tile[kk]))
+            w("tot *= D.gn[%d];" % kk)
+        w("*ntiles = tot;")
+        for n in self.stage_nodes:
+            nm = self.node_name(n)
+            f = n.func
+            nd = n.ndims
+            dims = ", ".join("(long long)((%s) - (%s) + 1)" % (
+                ctx.expr(d.upperBound, {}), ctx.expr(d.lowerBound, {}))
+                for d in f.domain)
+            box = ", ".join(str(e) for e in n._sm_ext)
+            w("{ long long dims[%d] = {%s}; int box[%d] = {%s};" % (
+                nd, dims, nd, box))
+            w("  D.tma_%s = pm_use_tma() && pm_make_tmap(&D.tm_%s, D.b_%s, "
+              "%d, dims, box, %d, %d); }" % (
+                  nm, nm, pg.fn(f), nd, f.typ.size(),
+                  1 if f.typ in (C.Float, C.Double) else 0))
+        w("return PM_OK;")
+        w.close()
+        w("")
+        w("static bool %s_attr = false;" % k)
+        w.open("static int launch_%s(pm_args& A, const size_t* wsoff, "
+               "cudaStream_t s)" % k)
+        w("%s_launch L; memset(&L, 0, sizeof(L));" % k)
+        w("L.nimg = 1;")
+        w("long long nt = 0;")
+        w("int st = %s(L.d0, A, wsoff, &nt); if (st) return st;" % fill)
+        w("if (nt == 0) return PM_OK;")
+        w("if (nt > 0x7fffffffLL) return PM_ERR_UNSUPPORTED;")
+        w.open("if (!%s_attr)" % k)
+        w("if (cudaFuncSetAttribute(%s, cudaFuncAttributeMaxDynamicShared"
+          "MemorySize, %d) != cudaSuccess) return PM_ERR_CUDA;" % (
+              k, plan.smem_bytes))
+        w("%s_attr = true;" % k)
+        w.close()
+        w("%s<<<(unsigned)nt, %d, %d, s>>>(L);" % (k, plan.threads,
+                                                  plan.smem_bytes))
+        w("return cudaGetLastError() == cudaSuccess ? PM_OK : PM_ERR_CUDA;")
+        w.close()
+        w("")
+        # batched: descriptors for all images in one upload
+        w.open("static int batch_%s(pm_args* As, const size_t* wsoffs, int "
+               "nslot, int n, char* pinned, char* ddesc, size_t* doff, "
+               "cudaStream_t s)" % k)
+        w("size_t off = (*doff + 63) & ~size_t(63);")
+        w("%s_desc* H = reinterpret_cast<%s_desc*>(pinned + off);" % (k, k))
+        w("long long base = 0;")
+        w.open("for (int i = 0; i < n; ++i)")
+        w("long long nt = 0;")
+        w("int st = %s(H[i], As[i], wsoffs + (size_t)i * nslot, &nt); if (st) "
+          "return st;" % fill)
+        w("H[i].tile_base = (int)base; base += nt;")
+        w.close()
+        w("*doff = off + sizeof(%s_desc) * n;" % k)
+        w("if (base == 0) return PM_OK;")
+        w("if (base > 0x7fffffffLL) return PM_ERR_UNSUPPORTED;")
+        w("if (cudaMemcpyAsync(ddesc + off, H, sizeof(%s_desc) * n, "
+          "cudaMemcpyHostToDevice, s) != cudaSuccess) return PM_ERR_CUDA;" % k)
+        w("cudaEventRecord(pm_batch_event, s);")
+        w("%s_launch L; memset(&L, 0, sizeof(L));" % k)
+        w("L.nimg = n; L.descs = reinterpret_cast<const %s_desc*>(ddesc + "
+          "off);" % k)
+        w("if (n == 1) L.d0 = H[0];")
+        w.open("if (!%s_attr)" % k)
+        w("if (cudaFuncSetAttribute(%s, cudaFuncAttributeMaxDynamicShared"
+          "MemorySize, %d) != cudaSuccess) return PM_ERR_CUDA;" % (
+              k, plan.smem_bytes))
+        w("%s_attr = true;" % k)
+        w.close()
+        w("%s<<<(unsigned)base, %d, %d, s>>>(L);" % (k, plan.threads,
+                                                    plan.smem_bytes))
+        w("return cudaGetLastError() == cudaSuccess ? PM_OK : PM_ERR_CUDA;")
+        w.close()
+        w("")
+        pg.launch_fns.append("launch_" + k)
+        pg.batch_fns.append("batch_" + k)
+        pg.desc_sizes.append("sizeof(%s_desc)" % k)
+
+
+# ---------------------------------------------------------------------------
+class ReductionGen(object):
+    """Init + privatized accumulation kernels of a Reduction group."""
+
+    def __init__(self, pg, group):
+        self.pg = pg
+        self.g = group
+        self.plan = group.plan
+        self.f = self.plan.func
+        self.k = "pm_%s_g%d" % (pg.pname, group.level_time)
+
+    def generate(self):
+        pg = self.pg
+        plan = self.plan
+        f = self.f
+        w = pg.w
+        k = self.k
+        fnm = pg.fn(f)
+        rvars = f.reductionVariables
+        nr = len(rvars)
+        nd = f.ndims
+        T = ctype(f.typ)
+        parts = body_parts(f)
+        reads = []
+        for cond, expr, red in parts:
+            for r in list(expr.collect(C.Reference)) + \
+                    (cond.collect(C.Reference) if cond is not None else []):
+                if all(r.objectRef is not q for q in reads) and \
+                        r.objectRef is not f:
+                    reads.append(r.objectRef)
+            for a in red.accumulate_ref.arguments:
+                for r in a.collect(C.Reference):
+                    if all(r.objectRef is not q for q in reads):
+                        reads.append(r.objectRef)
+        self.reads = reads
+        ops = set(red.op_type for _, _, red in parts)
+        if len(ops) != 1:
+            raise CodegenError("mixed reduction operators in %s" % f.name)
+        op = ops.pop()
+        self.op = op
+        pg.meta['groups'].append({
+            'kernel': k, 'kind': 'reduction', 'threads': plan.threads,
+            'smem': plan.smem_bytes, 'tile': plan.tile,
+            'stages': [f.name], 'privatized': plan.privatize,
+            'features': plan.features()})
+        w("// ---- group %d: reduction %s (tile %s, privatized %s)" % (
+            self.g.level_time, f.name, plan.tile, plan.privatize))
+        w.open("struct __align__(64) %s_desc" % k)
+        for prm in pg.params:
+            w("%s %s;" % (pg.ptype(prm), pg.pmap[prm]))
+        for x in reads:
+            w("const %s* b_%s;" % (ctype(x.typ), pg.fn(x)))
+        w("%s* b_%s;" % (T, fnm))
+        w("int glo[%d], ghi[%d], gn[%d];" % (nr, nr, nr))
+        w("int tile_base;")
+        w("long long ncells;")
+        w.close("};")
+        w.open("struct %s_launch" % k)
+        w("%s_desc d0;" % k)
+        w("const %s_desc* descs;" % k)
+        w("int nimg;")
+        w.close("};")
+        ident = self.identity()
+        # ---- init kernel: every cell to the default value ----
+        ctx0 = ExprCtx(w, 'device', pg.pmap, self.reader)
+        self.ctx = ctx0
+        w('extern "C" __global__ void __launch_bounds__(256) %s_init(const '
+          '__grid_constant__ %s_launch L)' % (k, k))
+        w.open("")
+        w.open("for (int im = 0; im < L.nimg; ++im)")
+        w("const %s_desc& D = (L.nimg == 1) ? L.d0 : L.descs[im];" % k)
+        pg.declare_params(w, "D")
+        w("%s* __restrict__ out = D.b_%s;" % (T, fnm))
+        pg.declare_domain(w, f, ctx0, True)
+        w.open("for (long long c = (long long)blockIdx.x * blockDim.x + "
+               "threadIdx.x; c < D.ncells; c += (long long)gridDim.x * "
+               "blockDim.x)")
+        w("long long rr = c;")
+        lv = _loop_vars(nd)
+        for d in range(nd - 1, -1, -1):
+            w("const int q%d = (int)(rr %% (d_%s_hi%d - d_%s_lo%d + 1)) + "
+              "d_%s_lo%d; rr /= (d_%s_hi%d - d_%s_lo%d + 1);" % (
+                  d, fnm, d, fnm, d, fnm, d, fnm, d, fnm, d))
+        bind = dict(zip(f.variables, lv))
+        w("out[c] = (%s)(%s);" % (T, ctx0.expr(f.default, bind)))
+        w.close()
+        w.close()
+        w.close()
+        w("")
+        # ---- accumulation kernel ----
+        w('extern "C" __global__ void __launch_bounds__(%d) %s(const '
+          '__grid_constant__ %s_launch L)' % (plan.threads, k, k))
+        w.open("")
+        w("extern __shared__ __align__(128) unsigned char pm_smem[];")
+        w("const int tile = blockIdx.x;")
+        w("const %s_desc* Dp = &L.d0;" % k)
+        w("if (L.nimg > 1) Dp = L.descs + pm_find_image(L.descs, L.nimg, "
+          "tile);")
+        w("const %s_desc& D = *Dp;" % k)
+        pg.declare_params(w, "D")
+        ctx = ExprCtx(w, 'device', pg.pmap, self.reader)
+        self.ctx = ctx
+        w("int rem = tile - D.tile_base;")
+        for d in range(nr - 1, 0, -1):
+            w("const int t%d = rem %% D.gn[%d]; rem /= D.gn[%d];" % (d, d, d))
+        w("const int t0 = rem;")
+        for d in range(nr):
+            w("const int a_lo%d = D.glo[%d] + t%d * %d;" % (d, d, d,
+                                                           plan.tile[d]))
+            w("const int a_hi%d = pm_imin(a_lo%d + %d, D.ghi[%d]);" % (
+                d, d, plan.tile[d] - 1, d))
+        pg.declare_domain(w, f, ctx, True)
+        for x in reads:
+            pg.declare_domain(w, x, ctx, True)
+            w("const %s* __restrict__ b_%s = D.b_%s;" % (ctype(x.typ),
+                                                         pg.fn(x), pg.fn(x)))
+        w("%s* __restrict__ out = D.b_%s;" % (T, fnm))
+        priv = plan.privatize
+        if priv:
+            # privatized box: union of target footprints of this tile
+            for d in range(nd):
+                w("int p_lo%d = 0x3fffffff, p_hi%d = -0x3fffffff;" % (d, d))
+            for fns in plan.target_fns:
+                for d, fn in enumerate(fns):
+                    if fn.kind == 'mono':
+                        a = ctx.expr(fn.expr, {fn.var: "a_lo%d" % fn.cdim})
+                        b = ctx.expr(fn.expr, {fn.var: "a_hi%d" % fn.cdim})
+                    elif fn.kind == 'const':
+                        a = b = ctx.expr(fn.expr, {})
+                    else:
+                        a, b = "d_%s_lo%d" % (fnm, d), "d_%s_hi%d" % (fnm, d)
+                    w("{ const int ea = %s, eb = %s; p_lo%d = pm_imin(p_lo%d, "
+                      "pm_imin(ea, eb)); p_hi%d = pm_imax(p_hi%d, pm_imax(ea, "
+                      "eb)); }" % (a, b, d, d, d, d))
+            for d in range(nd):
+                w("p_lo%d = pm_imax(p_lo%d, d_%s_lo%d); p_hi%d = pm_imin("
+                  "p_hi%d, d_%s_hi%d);" % (d, d, fnm, d, d, d, fnm, d))
+            ptot = 1
+            for e in plan.priv_ext:
+                ptot *= e
+            w("%s* acc = reinterpret_cast<%s*>(pm_smem);" % (T, T))
+            w("for (int i = threadIdx.x; i < %d; i += %d) acc[i] = %s;" % (
+                ptot, plan.threads, ident))
+            w("__syncthreads();")
+        # loop over the tile's reduction points
+        tot = 1
+        for t in plan.tile:
+            tot *= t
+        w.open("for (int i = threadIdx.x; i < %d; i += %d)" % (tot,
+                                                               plan.threads))
+        StencilGen.decompose(self, "i", plan.tile, "j")
+        lv = _loop_vars(nr)
+        for d in range(nr):
+            w("const int q%d = a_lo%d + j%d;" % (d, d, d))
+        w("if (%s) continue;" % " || ".join("q%d > a_hi%d" % (d, d)
+                                           for d in range(nr)))
+        rbind = dict(zip(rvars, lv))
+        for cond, expr, red in parts:
+            ctx.push()
+            tgt = red.accumulate_ref.arguments
+            tbind = dict(rbind)
+            for fv, ta in zip(f.variables, tgt):
+                tbind[fv] = _subst(ta, rbind)
+            w.open("")
+            for d, ta in enumerate(tgt):
+                w("const int c%d = %s;" % (d, ctx.expr(ta, rbind)))
+            inb = " && ".join("c%d >= d_%s_lo%d && c%d <= d_%s_hi%d" % (
+                d, fnm, d, d, fnm, d) for d in range(nd))
+            cc = ctx.cond(cond, tbind) if cond is not None else "true"
+            w.open("if ((%s) && (%s))" % (inb, cc))
+            val = ctx.expr(expr, rbind)
+            if priv:
+                sidx = " + ".join("(c%d - p_lo%d) * %d" % (
+                    d, d, _stride(plan.priv_ext, d)) for d in range(nd))
+                w("%s(&acc[%s], (%s)(%s));" % (self.atomic(), sidx, T, val))
+            else:
+                gidx = " + ".join("(long long)(c%d - d_%s_lo%d) * s_%s_%d" % (
+                    d, fnm, d, fnm, d) for d in range(nd))
+                w("%s(&out[%s], (%s)(%s));" % (self.atomic(), gidx, T, val))
+            w.close()
+            w.close()
+            ctx.pop()
+        w.close()
+        if priv:
+            w("__syncthreads();")
+            w.open("for (int i = threadIdx.x; i < %d; i += %d)" % (
+                ptot, plan.threads))
+            StencilGen.decompose(self, "i", plan.priv_ext, "j")
+            for d in range(nd):
+                w("const int c%d = p_lo%d + j%d;" % (d, d, d))
+            w("if (%s) continue;" % " || ".join("c%d > p_hi%d" % (d, d)
+                                               for d in range(nd)))
+            w("const %s v = acc[i];" % T)
+            w("if (v == %s) continue;" % ident)
+            gidx = " + ".join("(long long)(c%d - d_%s_lo%d) * s_%s_%d" % (
+                d, fnm, d, fnm, d) for d in range(nd))
+            w("%s(&out[%s], v);" % (self.atomic(), gidx))
+            w.close()
+        w.close()
+        w("")
+        self.gen_launcher()
+
+    def atomic(self):
+        return {C.Op.Sum: 'pm_atomic_add', C.Op.Mul: 'pm_atomic_mul',
+                C.Op.Min: 'pm_atomic_min', C.Op.Max: 'pm_atomic_max'}[self.op]
+
+    def identity(self):
+        T = self.f.typ
+        if self.op == C.Op.Sum:
+            return "(%s)0" % ctype(T)
+        if self.op == C.Op.Mul:
+            return "(%s)1" % ctype(T)
+        big = {C.Float: ("3.402823466e+38f", "-3.402823466e+38f"),
+               C.Double: ("1.7976931348623157e+308", "-1.7976931348623157e+308"),
+               C.Int: ("2147483647", "(-2147483647 - 1)"),
+               C.UInt: ("4294967295u", "0u")}
+        if T not in big:
+            raise CodegenError("Min/Max reduction of %s unsupported" % T)
+        return big[T][0] if self.op == C.Op.Min else big[T][1]
+
+    def reader(self, f, args, ctx):
+        pg = self.pg
+        key = (pg.fn(f), tuple(ctx.index(a) if not is_data_dependent(a)
+                                else ctx.expr(a, {}) for a in args))
+        hit = ctx.lookup(key)
+        if hit is not None:
+            return hit
+        t = ctx.temp()
+        pg.w("const %s %s = __ldg(b_%s + (%s));" % (
+            ctype(f.typ), t, pg.fn(f), pg.gindex(f, args, ctx)))
+        ctx.define(key, t)
+        return t
+
+    def gen_launcher(self):
+        pg = self.pg
+        plan = self.plan
+        f = self.f
+        w = pg.w
+        k = self.k
+        fnm = pg.fn(f)
+        nr = len(f.reductionVariables)
+        ctx = ExprCtx(w, 'device', pg.pmap, None)
+        fill = "fill_" + k
+        w.open("static int %s(%s_desc& D, const pm_args& A, const size_t* "
+               "wsoff, long long* ntiles)" % (fill, k))
+        pg.declare_params(w, "A")
+        for prm in pg.params:
+            w("D.%s = %s;" % (pg.pmap[prm], pg.pmap[prm]))
+        for x in self.reads:
+            w("D.b_%s = (const %s*)(%s);" % (pg.fn(x), ctype(x.typ),
+                                             pg.buf_expr(x)))
+        w("D.b_%s = (%s*)(%s);" % (fnm, ctype(f.typ), pg.buf_expr(f)))
+        w("D.ncells = 1;")
+        for d in f.domain:
+            w("D.ncells *= (long long)pm_nonneg((%s) - (%s) + 1);" % (
+                ctx.expr(d.upperBound, {}), ctx.expr(d.lowerBound, {})))
+        w("long long tot = 1;")
+        for i, d in enumerate(f.reductionDomain):
+            lo = ctx.expr(d.lowerBound, {})
+            hi = ctx.expr(d.upperBound, {})
+            w("D.glo[%d] = %s; D.ghi[%d] = %s;" % (i, lo, i, hi))
+            w("if (D.ghi[%d] < D.glo[%d]) { *ntiles = 0; return PM_OK; }" % (
+                i, i))
+            w("D.gn[%d] = (D.ghi[%d] - D.glo[%d] + %d) / %d; tot *= D.gn[%d];"
+              % (i, i, i, plan.tile[i], plan.tile[i], i))
+        w("*ntiles = tot;")
+        w("return PM_OK;")
+        w.close()
+        w("")
+        w("static bool %s_attr = false;" % k)
+        w.open("static int launch_%s(pm_args& A, const size_t* wsoff, "
+               "cudaStream_t s)" % k)
+        w("%s_launch L; memset(&L, 0, sizeof(L));" % k)
+        w("L.nimg = 1;")
+        w("long long nt = 0;")
+        w("int st = %s(L.d0, A, wsoff, &nt); if (st) return st;" % fill)
+        w("if (L.d0.ncells > 0) %s_init<<<(unsigned)pm_llmin((L.d0.ncells + "
+          "255) / 256, 148LL * 16), 256, 0, s>>>(L);" % k)
+        w("if (nt == 0) return cudaGetLastError() == cudaSuccess ? PM_OK : "
+          "PM_ERR_CUDA;")
+        w.open("if (!%s_attr)" % k)
+        w("if (cudaFuncSetAttribute(%s, cudaFuncAttributeMaxDynamicShared"
+          "MemorySize, %d) != cudaSuccess) return PM_ERR_CUDA;" % (
+              k, max(plan.smem_bytes, 16)))
+        w("%s_attr = true;" % k)
+        w.close()
+        w("%s<<<(unsigned)nt, %d, %d, s>>>(L);" % (k, plan.threads,
+                                                  max(plan.smem_bytes, 16)))
+        w("return cudaGetLastError() == cudaSuccess ? PM_OK : PM_ERR_CUDA;")
+        w.close()
+        w("")
+        w.open("static int batch_%s(pm_args* As, const size_t* wsoffs, int "
+               "nslot, int n, char* pinned, char* ddesc, size_t* doff, "
+               "cudaStream_t s)" % k)
+        w("size_t off = (*doff + 63) & ~size_t(63);")
+        w("%s_desc* H = reinterpret_cast<%s_desc*>(pinned + off);" % (k, k))
+        w("long long base = 0, cells = 0;")
+        w.open("for (int i = 0; i < n; ++i)")
+        w("long long nt = 0;")
+        w("int st = %s(H[i], As[i], wsoffs + (size_t)i * nslot, &nt); if (st) "
+          "return st;" % fill)
+        w("H[i].tile_base = (int)base; base += nt; cells += H[i].ncells;")
+        w.close()
+        w("*doff = off + sizeof(%s_desc) * n;" % k)
+        w("if (cudaMemcpyAsync(ddesc + off, H, sizeof(%s_desc) * n, "
+          "cudaMemcpyHostToDevice, s) != cudaSuccess) return PM_ERR_CUDA;" % k)
+        w("cudaEventRecord(pm_batch_event, s);")
+        w("%s_launch L; memset(&L, 0, sizeof(L));" % k)
+        w("L.nimg = n; L.descs = reinterpret_cast<const %s_desc*>(ddesc + "
+          "off);" % k)
+        w("if (n == 1) L.d0 = H[0];")
+        w("if (cells > 0) %s_init<<<(unsigned)pm_llmin((cells + 255) / 256, "
+          "148LL * 16), 256, 0, s>>>(L);" % k)
+        w("if (base == 0) return cudaGetLastError() == cudaSuccess ? PM_OK : "
+          "PM_ERR_CUDA;")
+        w("if (base > 0x7fffffffLL) return PM_ERR_UNSUPPORTED;")
+        w.open("if (!%s_attr)" % k)
+        w("if (cudaFuncSetAttribute(%s, cudaFuncAttributeMaxDynamicShared"
+          "MemorySize, %d) != cudaSuccess) return PM_ERR_CUDA;" % (
+              k, max(plan.smem_bytes, 16)))
+        w("%s_attr = true;" % k)
+        w.close()
+        w("%s<<<(unsigned)base, %d, %d, s>>>(L);" % (k, plan.threads,
+                                                    max(plan.smem_bytes, 16)))
+        w("return cudaGetLastError() == cudaSuccess ? PM_OK : PM_ERR_CUDA;")
+        w.close()
+        w("")
+        pg.launch_fns.append("launch_" + k)
+        pg.batch_fns.append("batch_" + k)
+        pg.desc_sizes.append("sizeof(%s_desc)" % k)
+
+
+def _stride(ext, d):
+    s = 1
+    for e in ext[d + 1:]:
+        s *= e
+    return s
+
+
+# ---------------------------------------------------------------------------
+class ConstGen(object):
+    """Host tabulation + upload of a const function."""
+
+    def __init__(self, pg, group):
+        self.pg = pg
+        self.g = group
+        self.f = group.plan.func
+
+    def generate(self):
+        pg = self.pg
+        f = self.f
+        fnm = pg.fn(f)
+        hw = pg.hw
+        w = pg.w
+        reads = []
+        for r in f.getObjects(C.Reference):
+            o = r.objectRef
+            if o is not f and all(o is not q for q in reads):
+                reads.append(o)
+        for o in reads:
+            if not (isinstance(o, C.Image) or o.is_const_func):
+                raise CodegenError("const function %s reads non-const %s" % (
+                    f.name, o.name))
+        self.reads = reads
+        pg.meta['groups'].append({'kernel': None, 'kind': 'const',
+                                  'stages': [f.name]})
+        # ---- host C++ tabulation (compiled by g++ with the reference's
+        # flags) ----
+        hparams = ", ".join(["%s %s" % (pg.ptype(q), pg.pmap[q])
+                             for q in pg.params] +
+                            ["const %s* b_%s" % (ctype(o.typ), pg.fn(o))
+                             for o in reads] +
+                            ["%s* out" % ctype(f.typ)])
+        hw('extern "C" void pm_const_%s_%s(%s)' % (pg.pname, fnm, hparams))
+        hw.open("")
+        ctx = ExprCtx(hw, 'host', pg.pmap, self.host_reader)
+        self.ctx = ctx
+        for o in reads + [f]:
+            pg.declare_domain(hw, o, ctx, True)
+        nd = f.ndims
+        lv = _loop_vars(nd)
+        for d in range(nd):
+            hw.open("for (int q%d = d_%s_lo%d; q%d <= d_%s_hi%d; ++q%d)" % (
+                d, fnm, d, d, fnm, d, d))
+        ctx.push()
+        bind = dict(zip(f.variables, lv))
+        hw("%s v = 0;" % ctype(f.typ))
+        parts = body_parts(f)
+        if len(parts) == 1 and parts[0][0] is None:
+            hw("v = (%s)(%s);" % (ctype(f.typ), ctx.expr(parts[0][1], bind)))
+        else:
+            first = True
+            for cond, expr, red in reversed(parts):
+                ctx.push()
+                c = ctx.cond(cond, bind) if cond is not None else "true"
+                hw.open("%sif (%s)" % ("" if first else "else ", c))
+                hw("v = (%s)(%s);" % (ctype(f.typ), ctx.expr(expr, bind)))
+                hw.close()
+                ctx.pop()
+                first = False
+        idx = " + ".join("(long long)(q%d - d_%s_lo%d) * s_%s_%d" % (
+            d, fnm, d, fnm, d) for d in range(nd))
+        hw("out[%s] = v;" % idx)
+        ctx.pop()
+        for d in range(nd):
+            hw.close()
+        hw.close()
+        hw("")
+        # ---- device-side: cached upload -----------------------------------
+        w('extern "C" void pm_const_%s_%s(%s);' % (pg.pname, fnm, hparams))
+        dctx = ExprCtx(w, 'device', pg.pmap, None)
+        ext = " * ".join("(size_t)pm_nonneg((%s) - (%s) + 1)" % (
+            dctx.expr(d.upperBound, {}), dctx.expr(d.lowerBound, {}))
+            for d in f.domain)
+        w("static std::vector<char> ctab_key_%s;" % fnm)
+        w("static std::vector<char> ctab_host_%s;" % fnm)
+        w("static pm_arena ctab_dev_%s;" % fnm)
+        w.open("static int launch_const_%s(pm_args& A, const size_t* wsoff, "
+               "cudaStream_t s)" % fnm)
+        pg.declare_params(w, "A")
+        w("std::vector<char> key;")
+        for q in pg.params:
+            w("{ const char* p = (const char*)&%s; key.insert(key.end(), p, p "
+              "+ sizeof(%s)); }" % (pg.pmap[q], pg.pmap[q]))
+        hostbufs = []
+        for o in reads:
+            on = pg.fn(o)
+            oext = " * ".join("(size_t)pm_nonneg((%s) - (%s) + 1)" % (
+                dctx.expr(d.upperBound, {}), dctx.expr(d.lowerBound, {}))
+                for d in o.domain)
+            w("std::vector<char> hb_%s((size_t)%d * %s);" % (on, o.typ.size(),
+                                                             oext))
+            if isinstance(o, C.Image):
+                w("if (!hb_%s.empty()) { if (pm_host_ptr(A.b_%s)) memcpy("
+                  "hb_%s.data(), A.b_%s, hb_%s.size()); else if (cudaMemcpy"
+                  "Async(hb_%s.data(), A.b_%s, hb_%s.size(), cudaMemcpyDevice"
+                  "ToHost, s) != cudaSuccess || cudaStreamSynchronize(s) != "
+                  "cudaSuccess) return PM_ERR_CUDA; }" % (
+                      on, on, on, on, on, on, on, on))
+            else:
+                w("hb_%s = ctab_host_%s;" % (on, on))
+            w("key.insert(key.end(), hb_%s.begin(), hb_%s.end());" % (on, on))
+            hostbufs.append("(const %s*)hb_%s.data()" % (ctype(o.typ), on))
+        w("const size_t nb = (size_t)%d * %s;" % (f.typ.size(), ext))
+        w.open("if (key != ctab_key_%s || ctab_host_%s.size() != nb)" % (
+            fnm, fnm))
+        w("ctab_host_%s.assign(nb, 0);" % fnm)
+        args = [pg.pmap[q] for q in pg.params] + hostbufs + \
+            ["(%s*)ctab_host_%s.data()" % (ctype(f.typ), fnm)]
+        w("pm_const_%s_%s(%s);" % (pg.pname, fnm, ", ".join(args)))
+        w("void* d = nullptr;")
+        w("if (pm_arena_get(&ctab_dev_%s, nb, &d)) return PM_ERR_CUDA;" % fnm)
+        w("if (cudaMemcpy(d, ctab_host_%s.data(), nb, cudaMemcpyHostToDevice)"
+          " != cudaSuccess) return PM_ERR_CUDA;" % fnm)
+        w("ctab_key_%s = key;" % fnm)
+        w.close()
+        w("void* d = nullptr;")
+        w("if (pm_arena_get(&ctab_dev_%s, nb, &d)) return PM_ERR_CUDA;" % fnm)
+        w("ctab_ptr_%s = (char*)d;" % fnm)
+        w("return PM_OK;")
+        w.close()
+        w("")
+        pg.const_ptrs.append(fnm)
+        pg.launch_fns.append("launch_const_" + fnm)
+        pg.batch_fns.append("batch_const_" + fnm)
+        w.open("static int batch_const_%s(pm_args* As, const size_t* wsoffs, "
+               "int nslot, int n, char* pinned, char* ddesc, size_t* doff, "
+               "cudaStream_t s)" % fnm)
+        w("for (int i = 1; i < n; ++i) if (memcmp(&As[i], &As[0], "
+          "sizeof(pm_args)) != 0) { /* tables depend on parameters only */ }")
+        w("return launch_const_%s(As[0], wsoffs, s);" % fnm)
+        w.close()
+        w("")
+
+    def host_reader(self, f, args, ctx):
+        pg = self.pg
+        t = ctx.temp()
+        idx = pg.gindex(f, args, ctx)
+        ctx.w("const %s %s = b_%s[%s];" % (ctype(f.typ), t, pg.fn(f), idx))
+        return t
+
+
+# ---------------------------------------------------------------------------
+def generate_code_for_pipeline(pipeline):
+    pg = PipelineGen(pipeline)
+    pg.slot_of = getattr(pipeline, '_storage_assign', {})
+    pg.nslots = len(getattr(pipeline, '_storage_slots', []))
+    pg.launch_fns = []
+    pg.batch_fns = []
+    pg.desc_sizes = []
+    pg.const_ptrs = []
+    # const tables are addressed through ctab pointers set by their launch
+    pg.buf_expr_orig = pg.buf_expr
+    body = W()
+    pg_w = pg.w
+    pg.w = body
+    # generate groups into `body` first so helper declarations can precede
+    for g in pipeline.groups:
+        plan = g.plan
+        if plan.kind == 'stencil':
+            StencilGen(pg, g).generate()
+        elif plan.kind == 'reduction':
+            ReductionGen(pg, g).generate()
+        else:
+            ConstGen(pg, g).generate()
+    pg.w = pg_w
+    w = pg.w
+    w("// pipeline %s -- generated by polymage_b200 for sm_100a" %
+      pipeline.name)
+    w('#include "pm_runtime.cuh"')
+    w("#include <vector>")
+    w("")
+    w("__device__ unsigned pm_err_word;")
+    w("static int pm_status = 0;")
+    w("static cudaEvent_t pm_batch_event = nullptr;")
+    w("static inline long long pm_nonneg(long long v) { return v < 0 ? 0 : v;"
+      " }")
+    w("static inline long long pm_llmin(long long a, long long b) { return a "
+      "< b ? a : b; }")
+    w("static inline long long pm_llmax(long long a, long long b) { return a "
+      "> b ? a : b; }")
+    w("static inline int isl_min_i(int a, int b) { return a < b ? a : b; }")
+    w("static inline int isl_max_i(int a, int b) { return a > b ? a : b; }")
+    w("static bool pm_use_tma() { static int v = -1; if (v < 0) { const char*"
+      " e = getenv(\"PM_DISABLE_TMA\"); v = (e && e[0] == '1') ? 0 : 1; } "
+      "return v == 1; }")
+    w("static bool pm_host_ptr(const void* p) { cudaPointerAttributes a; if "
+      "(cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError();"
+      " return true; } return a.type != cudaMemoryTypeDevice && a.type != "
+      "cudaMemoryTypeManaged; }")
+    for fnm in pg.const_ptrs:
+        w("static char* ctab_ptr_%s = nullptr;" % fnm)
+    w("")
+    pg.gen_args_struct()
+    pg.gen_validate()
+    pg.gen_workspace()
+    w.lines.extend(body.lines)
+    w("static size_t pm_batch_desc_bytes(int n) { return (size_t)n * (%s) + "
+      "64 * %d; }" % (" + ".join(pg.desc_sizes) or "0",
+                      len(pg.desc_sizes) + 1))
+    w("")
+    pg.gen_entries()
+    header = pg.gen_header()
+    return CudaModule(pipeline.name, w.text(), pg.host_text(), header,
+                      pg.meta)

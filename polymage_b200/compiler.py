@@ -1,0 +1,47 @@
+"""Compiler entry point (sandbox/compiler.py:33-80).
+
+``buildPipeline`` keeps the reference's keyword arguments and defaults:
+``group_size`` 5, ``tile_sizes`` [16, 16, 16], ``size_threshold`` 200*200,
+and ``optimize_storage`` implying ``flatten_scratchpad``.  Options may also
+carry CUDA-target settings as ``"name=value"`` strings or ``(name, value)``
+tuples: ``threads`` (CTA size), ``inline_budget`` (register-recompute budget
+per consumer point), ``smem_budget`` (bytes per CTA), ``tile`` (tile sizes
+overriding ``tile_sizes``), ``materialize`` (list of function names kept in
+shared memory), ``no_stage`` (never stage inputs in shared memory),
+``no_privatize`` (reductions accumulate straight into HBM),
+``no_storage_reuse``.
+"""
+
+from .pipe import Pipeline
+
+
+def buildPipeline(outputs,
+                  param_estimates=[],
+                  param_constraints=[],
+                  grouping=[],
+                  group_size=None,
+                  inline_directives=[],
+                  tile_sizes=[],
+                  size_threshold=None,
+                  pipe_name=None,
+                  options=[]):
+    outputs = list(dict.fromkeys(outputs))
+    if group_size is None:
+        group_size = 5
+    if not tile_sizes:
+        tile_sizes = [16, 16, 16]
+    if size_threshold is None:
+        size_threshold = 200 * 200
+    options = list(options)
+    if 'optimize_storage' in options and 'flatten_scratchpad' not in options:
+        options.append('flatten_scratchpad')
+    return Pipeline(_outputs=outputs,
+                    _param_estimates=param_estimates,
+                    _param_constraints=param_constraints,
+                    _grouping=grouping,
+                    _group_size=group_size,
+                    _inline_directives=inline_directives,
+                    _tile_sizes=tile_sizes,
+                    _size_threshold=size_threshold,
+                    _name=pipe_name,
+                    _options=options)

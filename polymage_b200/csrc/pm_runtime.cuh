@@ -1,0 +1,323 @@
+// pm_runtime.cuh -- device and host support code included by every pipeline
+// translation unit that the polymage_b200 code generator emits.
+//
+// Device side: mbarrier and TMA (cp.async.bulk.tensor, no multicast)
+// wrappers for sm_100a, bounded waits that record a timeout in the module's
+// error word instead of spinning forever, small integer helpers and atomics
+// for reductions.
+// Host side: tensor-map encoding through the driver entry point (no link
+// against libcuda), a per-device workspace arena reused across calls, and
+// status codes shared by all generated entry points.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+#include <math.h>
+#include <mutex>
+
+#define PM_OK 0
+#define PM_ERR_PARAMS 1       // parameter values outside the spec's bounds
+#define PM_ERR_CUDA 2         // a CUDA call failed
+#define PM_ERR_KERNEL 3       // a kernel reported an error (timeout, overflow)
+#define PM_ERR_UNSUPPORTED 4  // request outside what this build supports
+
+// bits of the device error word
+#define PM_KERR_TMA_TIMEOUT 1u
+#define PM_KERR_REGION 2u
+#define PM_KERR_QUEUE 4u
+
+#ifndef PM_WAIT_LIMIT
+#define PM_WAIT_LIMIT (1 << 24)
+#endif
+
+// ---------------------------------------------------------------------------
+// device helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int pm_imin(int a, int b) { return a < b ? a : b; }
+__device__ __forceinline__ int pm_imax(int a, int b) { return a > b ? a : b; }
+__device__ __forceinline__ int pm_clampi(int v, int lo, int hi) {
+  return v < lo ? lo : (v > hi ? hi : v);
+}
+__host__ __device__ __forceinline__ int pm_floordiv(int a, int b) {
+  int q = a / b;
+  return (q * b != a && ((a < 0) != (b < 0))) ? q - 1 : q;
+}
+
+// |v| with the argument's own precision (what C++ std::abs resolves to)
+__host__ __device__ __forceinline__ int pm_abs(int v) { return v < 0 ? -v : v; }
+__host__ __device__ __forceinline__ long long pm_abs(long long v) { return v < 0 ? -v : v; }
+__host__ __device__ __forceinline__ unsigned pm_abs(unsigned v) { return v; }
+__host__ __device__ __forceinline__ unsigned long long pm_abs(unsigned long long v) { return v; }
+__host__ __device__ __forceinline__ float pm_abs(float v) { return fabsf(v); }
+__host__ __device__ __forceinline__ double pm_abs(double v) { return fabs(v); }
+
+__device__ __forceinline__ uint32_t pm_smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void pm_mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(pm_smem_addr(bar)),
+               "r"(count)
+               : "memory");
+}
+
+// make the initialized barrier visible to the async (TMA) proxy
+__device__ __forceinline__ void pm_fence_barrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void pm_mbar_arrive_expect_tx(uint64_t* bar,
+                                                         uint32_t bytes) {
+  asm volatile(
+      "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+          pm_smem_addr(bar)),
+      "r"(bytes)
+      : "memory");
+}
+
+__device__ __forceinline__ bool pm_mbar_try_wait(uint64_t* bar, uint32_t phase) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(pm_smem_addr(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+
+// Wait for a barrier phase with an iteration limit; on timeout set the error
+// word and report failure (the caller then skips its compute).
+__device__ __forceinline__ bool pm_mbar_wait(uint64_t* bar, uint32_t phase,
+                                             unsigned* err) {
+  for (int it = 0; it < PM_WAIT_LIMIT; ++it) {
+    if (pm_mbar_try_wait(bar, phase)) return true;
+  }
+  if (err) atomicOr(err, PM_KERR_TMA_TIMEOUT);
+  return false;
+}
+
+// Tiled TMA loads into this CTA's shared memory; completion is signalled on
+// `bar` by transaction bytes.  The innermost coordinate must be 16-byte
+// aligned (the callers round it down).
+__device__ __forceinline__ void pm_tma_load_1d(void* dst, const CUtensorMap* m,
+                                               uint64_t* bar, int c0) {
+  asm volatile(
+      "cp.async.bulk.tensor.1d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2}], [%3];" ::"r"(pm_smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(m)), "r"(c0), "r"(pm_smem_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ void pm_tma_load_2d(void* dst, const CUtensorMap* m,
+                                               uint64_t* bar, int c0, int c1) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(pm_smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(m)), "r"(c0), "r"(c1),
+      "r"(pm_smem_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ void pm_tma_load_3d(void* dst, const CUtensorMap* m,
+                                               uint64_t* bar, int c0, int c1,
+                                               int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(pm_smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(m)), "r"(c0), "r"(c1), "r"(c2),
+      "r"(pm_smem_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ void pm_tma_load_4d(void* dst, const CUtensorMap* m,
+                                               uint64_t* bar, int c0, int c1,
+                                               int c2, int c3) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(pm_smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(m)), "r"(c0), "r"(c1), "r"(c2), "r"(c3),
+      "r"(pm_smem_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ void pm_tma_load_5d(void* dst, const CUtensorMap* m,
+                                               uint64_t* bar, int c0, int c1,
+                                               int c2, int c3, int c4) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(pm_smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(m)), "r"(c0), "r"(c1), "r"(c2), "r"(c3),
+      "r"(c4), "r"(pm_smem_addr(bar))
+      : "memory");
+}
+
+// ---- atomics used by reductions ------------------------------------------
+__device__ __forceinline__ void pm_atomic_add(float* p, float v) { atomicAdd(p, v); }
+__device__ __forceinline__ void pm_atomic_add(double* p, double v) { atomicAdd(p, v); }
+__device__ __forceinline__ void pm_atomic_add(int* p, int v) { atomicAdd(p, v); }
+__device__ __forceinline__ void pm_atomic_add(unsigned* p, unsigned v) { atomicAdd(p, v); }
+__device__ __forceinline__ void pm_atomic_add(long long* p, long long v) {
+  atomicAdd(reinterpret_cast<unsigned long long*>(p), (unsigned long long)v);
+}
+__device__ __forceinline__ void pm_atomic_add(unsigned long long* p,
+                                              unsigned long long v) {
+  atomicAdd(p, v);
+}
+__device__ __forceinline__ void pm_atomic_min(int* p, int v) { atomicMin(p, v); }
+__device__ __forceinline__ void pm_atomic_max(int* p, int v) { atomicMax(p, v); }
+__device__ __forceinline__ void pm_atomic_min(unsigned* p, unsigned v) { atomicMin(p, v); }
+__device__ __forceinline__ void pm_atomic_max(unsigned* p, unsigned v) { atomicMax(p, v); }
+__device__ __forceinline__ void pm_atomic_min(float* p, float v) {
+  int* ip = reinterpret_cast<int*>(p);
+  int old = *ip;
+  while (__int_as_float(old) > v) {
+    int prev = atomicCAS(ip, old, __float_as_int(v));
+    if (prev == old) break;
+    old = prev;
+  }
+}
+__device__ __forceinline__ void pm_atomic_max(float* p, float v) {
+  int* ip = reinterpret_cast<int*>(p);
+  int old = *ip;
+  while (__int_as_float(old) < v) {
+    int prev = atomicCAS(ip, old, __float_as_int(v));
+    if (prev == old) break;
+    old = prev;
+  }
+}
+__device__ __forceinline__ void pm_atomic_mul(float* p, float v) {
+  int* ip = reinterpret_cast<int*>(p);
+  int old = *ip;
+  while (true) {
+    int prev = atomicCAS(ip, old, __float_as_int(__int_as_float(old) * v));
+    if (prev == old) break;
+    old = prev;
+  }
+}
+__device__ __forceinline__ void pm_atomic_mul(int* p, int v) {
+  int old = *p;
+  while (true) {
+    int prev = atomicCAS(p, old, old * v);
+    if (prev == old) break;
+    old = prev;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host helpers
+// ---------------------------------------------------------------------------
+typedef CUresult (*pm_encode_tiled_fn)(CUtensorMap*, CUtensorMapDataType,
+                                       cuuint32_t, void*, const cuuint64_t*,
+                                       const cuuint64_t*, const cuuint32_t*,
+                                       const cuuint32_t*, CUtensorMapInterleave,
+                                       CUtensorMapSwizzle,
+                                       CUtensorMapL2promotion,
+                                       CUtensorMapFloatOOBfill);
+
+static pm_encode_tiled_fn pm_get_encode_fn() {
+  static pm_encode_tiled_fn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, []() {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault,
+                                &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<pm_encode_tiled_fn>(p);
+  });
+  return fn;
+}
+
+static CUtensorMapDataType pm_tma_dtype(int elem_size, int is_float) {
+  switch (elem_size) {
+    case 1: return CU_TENSOR_MAP_DATA_TYPE_UINT8;
+    case 2: return CU_TENSOR_MAP_DATA_TYPE_UINT16;
+    case 4: return is_float ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                            : CU_TENSOR_MAP_DATA_TYPE_UINT32;
+    default: return is_float ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                             : CU_TENSOR_MAP_DATA_TYPE_INT64;
+  }
+}
+
+// Encode a tiled tensor map over a dense row-major array.  `dims` and `box`
+// are given outermost first (C order); returns false when the TMA
+// preconditions do not hold (alignment, box limits), in which case the
+// kernel falls back to cooperative loads.
+static bool pm_make_tmap(CUtensorMap* m, const void* base, int rank,
+                         const long long* dims, const int* box, int elem_size,
+                         int is_float) {
+  memset(m, 0, sizeof(*m));
+  pm_encode_tiled_fn fn = pm_get_encode_fn();
+  if (!fn || rank < 1 || rank > 5) return false;
+  if ((reinterpret_cast<uintptr_t>(base) & 15) != 0) return false;
+  cuuint64_t gdim[5], gstride[5];
+  cuuint32_t bdim[5], estr[5];
+  long long stride = elem_size;
+  for (int i = 0; i < rank; ++i) {
+    int c = rank - 1 - i;  // reverse to innermost-first
+    if (dims[c] <= 0 || box[c] <= 0 || box[c] > 256) return false;
+    gdim[i] = (cuuint64_t)dims[c];
+    bdim[i] = (cuuint32_t)box[c];
+    estr[i] = 1;
+    if (i > 0) {
+      if (stride % 16 != 0) return false;
+      gstride[i - 1] = (cuuint64_t)stride;
+    }
+    stride *= dims[c];
+  }
+  if ((bdim[0] * elem_size) % 16 != 0) return false;
+  CUresult r = fn(m, pm_tma_dtype(elem_size, is_float), (cuuint32_t)rank,
+                  const_cast<void*>(base), gdim, gstride, bdim, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+// Workspace arena: one device allocation per device, grown on demand and
+// reused across calls (the device counterpart of the reference's pool
+// allocator, sandbox/memory_allocation/simple_pool_allocator.cpp).
+struct pm_arena {
+  void* ptr[64];
+  size_t cap[64];
+};
+
+static int pm_arena_get(pm_arena* a, size_t bytes, void** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+    return PM_ERR_CUDA;
+  if (bytes == 0) bytes = 256;
+  if (a->cap[dev] < bytes) {
+    if (a->ptr[dev]) {
+      cudaDeviceSynchronize();
+      cudaFree(a->ptr[dev]);
+    }
+    a->ptr[dev] = nullptr;
+    a->cap[dev] = 0;
+    size_t want = bytes + bytes / 8;
+    if (cudaMalloc(&a->ptr[dev], want) != cudaSuccess) {
+      cudaGetLastError();
+      return PM_ERR_CUDA;
+    }
+    a->cap[dev] = want;
+  }
+  *out = a->ptr[dev];
+  return PM_OK;
+}
+
+static inline size_t pm_align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Binary search of a tile index in a batch's tile prefix (descriptors carry
+// their first tile); used by batched launches.
+template <typename D>
+__device__ __forceinline__ int pm_find_image(const D* descs, int n, int tile) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (descs[mid].tile_base <= tile) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
