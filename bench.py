@@ -1,0 +1,334 @@
+#!/usr/bin/env python
+"""Benchmark of the PolyMage unsharp-mask pipeline on B200.
+
+Workload (one step): unsharp mask over one 3-channel 4096x4096 float32
+image, values U[0,1) from seed 0 with the reference's 2-pixel zero ghost
+zone, weight 3, threshold 0.001; one launch of the fused group kernel.
+
+Reported (one JSON line, rank 0):
+  value     MPix/s of the whole job with inputs resident in HBM, timed with
+            CUDA events over exactly --steps steps (max over ranks)
+  e2e       the same metric through the reference's C ABI
+            (``pipeline_unsharp`` on pinned host buffers: host->device copy
+            of the input and device->host copy of the result every step)
+  roofline  compulsory bytes per launch / mean kernel time vs the measured
+            HBM copy bandwidth
+  cpu_baseline  the reference's own generated C++ (pipeline_mask, OpenMP on
+            all host cores) on a bounded sample of the same workload
+  clocks    SM clocks and throttle reasons sampled during the timed region
+
+``--impl reference`` times the reference's CPU implementation alone.
+Multi-GPU (torchrun): every rank runs its own image (replicas, weak
+scaling); no collective is on the data path.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+R = C = 4096
+THRESHOLD, WEIGHT = 0.001, 3.0
+TILE = (32, 128)
+IN_BYTES = 3 * (R + 4) * (C + 4) * 4
+OUT_BYTES = 3 * R * C * 4
+ALG_BYTES = IN_BYTES + OUT_BYTES          # compulsory bytes per step
+D2H_BYTES = 3 * (R - 1) * (C - 1) * 4     # points the pipeline writes
+METRIC = "MPix/s, unsharp mask 3x4096x4096 float32 (w=3, thr=0.001)"
+WORKLOAD = "unsharp_mask 3x4096x4096 float32 w=3 threshold=0.001"
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    return ws, rank
+
+
+# ---------------------------------------------------------------------------
+class Clocks(object):
+    """nvidia-smi sampler running while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,"
+         "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "50"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                universal_newlines=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [],
+                    "samples": 0}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(smax)) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def cpu_baseline(budget_s=3.0):
+    """The reference's own generated C++ (pipeline_mask from
+    sandbox/video_demo/unsharp_polymage.cpp, OpenMP on all host threads) on
+    the same image size; its input is the uint8 image it is written for."""
+    threads = os.cpu_count()
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    import oracle.ref as ref
+    if not ref.available("unsharp"):
+        return None
+    rng = np.random.default_rng(0)
+    u8 = rng.integers(0, 256, (R + 4, C + 4, 3), dtype=np.uint8)
+    out = np.zeros((R, C, 3), np.float32)
+    ref.ref_unsharp(u8, THRESHOLD, WEIGHT, out)       # warm-up
+    ts = []
+    t_end = time.perf_counter() + budget_s
+    while time.perf_counter() < t_end or len(ts) < 3:
+        t0 = time.perf_counter()
+        ref.ref_unsharp(u8, THRESHOLD, WEIGHT, out)
+        ts.append(time.perf_counter() - t0)
+    best = min(ts)
+    return {"value": R * C / best / 1e6, "unit": "MPix/s", "cores": threads,
+            "kind": "reference",
+            "sample": "%d full 3x%dx%d images through pipeline_mask "
+                      "(reference generated C++, uint8 interleaved input), "
+                      "best of %d" % (len(ts), R, C, len(ts))}
+
+
+def run_reference_arm(args):
+    ws, rank = _dist()
+    if rank != 0:
+        return 0
+    threads = os.cpu_count()
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    import oracle.ref as ref
+    if not ref.available("unsharp"):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/libref_unsharp.so not built"}))
+        return 0
+    # each step: a 256-row band of the image (a bounded sample)
+    band = 256
+    rng = np.random.default_rng(0)
+    u8 = rng.integers(0, 256, (band + 4, C + 4, 3), dtype=np.uint8)
+    out = np.zeros((band, C, 3), np.float32)
+    for _ in range(args.warmup):
+        ref.ref_unsharp(u8, THRESHOLD, WEIGHT, out)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ref.ref_unsharp(u8, THRESHOLD, WEIGHT, out)
+    dt = time.perf_counter() - t0
+    v = args.steps * band * C / dt / 1e6
+    line = {"metric": METRIC, "value": v, "unit": "MPix/s", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic uint8 U{0..255} (the reference variant's "
+                    "input type), seed 0",
+            "config": {"workload": WORKLOAD, "sample": "3x%dx%d band per "
+                       "step" % (band, C)},
+            "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "MPix/s", "cores": threads,
+                             "kind": "reference",
+                             "sample": "%d steps of a 3x%dx%d band through "
+                                       "pipeline_mask" % (args.steps, band,
+                                                          C)},
+            "e2e": {"value": v, "unit": "MPix/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+def _load_traffic(kernel):
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    v = d.get(kernel)
+    return float(v["bytes_per_launch"]) if v else None
+
+
+def run(args):
+    import torch
+    import torch.distributed as dist
+    ws, rank = _dist()
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if ws > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=dev)
+    from polymage_b200.apps.unsharp_mask import build_unsharp
+    import oracle.unsharp as OU
+
+    cp = build_unsharp(tile_sizes=TILE).build()
+    kernel = cp.module.meta['groups'][0]['kernel']
+    prm = {'R': R, 'C': C, 'threshold': THRESHOLD, 'weight': WEIGHT}
+    host_in = OU.make_input(R, C, seed=0)
+    d_in = torch.from_numpy(host_in).to(dev)
+    d_out = torch.zeros((3, R, C), dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        cp.run_dev(prm, {'img': d_in}, {'mask': d_out},
+                   stream=stream.cuda_stream)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize(dev)
+    cp.check()
+
+    # --- timed region: exactly --steps steps, inputs resident in HBM -------
+    clocks = Clocks(torch.cuda.current_device()) if rank == 0 else None
+    if clocks:
+        clocks.start()
+        time.sleep(0.3)
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    ev = [(torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for i in range(args.steps):
+        ev[i][0].record(stream)
+        step()
+        ev[i][1].record(stream)
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    if ws > 1:
+        dist.barrier()
+    clk = clocks.stop() if clocks else None
+    cp.check()
+    elapsed_ms = t0.elapsed_time(t1)
+    kern_ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
+    if ws > 1:
+        t = torch.tensor([elapsed_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    value = ws * args.steps * R * C / (elapsed_ms / 1e3) / 1e6
+
+    # --- end to end through the reference C ABI (host buffers) -------------
+    pin_in = torch.empty(host_in.shape, dtype=torch.float32,
+                         pin_memory=True)
+    pin_in.numpy()[...] = host_in
+    pin_out = torch.zeros((3, R, C), dtype=torch.float32, pin_memory=True)
+    a_in, a_out = pin_in.numpy(), pin_out.numpy()
+    e2e_steps = max(3, min(args.steps, 20))
+    for _ in range(2):
+        cp.run_host(prm, {'img': a_in}, {'mask': a_out})
+    if ws > 1:
+        dist.barrier()
+    s0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        cp.run_host(prm, {'img': a_in}, {'mask': a_out})
+    e2e_s = time.perf_counter() - s0
+    if ws > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = ws * e2e_steps * R * C / e2e_s / 1e6
+
+    if rank == 0:
+        peak, peak_kind = _peaks()
+        achieved = ALG_BYTES / (kern_ms / 1e3) / 1e9
+        traffic = _load_traffic(kernel)
+        line = {
+            "metric": METRIC, "value": value, "unit": "MPix/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": elapsed_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: U[0,1) seed 0, 2-px zero ghost zone",
+            "config": {"workload": WORKLOAD, "tile": list(TILE),
+                       "kernel": kernel,
+                       "l2": "inputs larger than L2 (201.7 MB in + 201.3 MB "
+                             "out per step vs 126 MB L2)",
+                       "parallelism": "replicas x%d" % ws},
+            "e2e": {"value": e2e, "unit": "MPix/s",
+                    "h2d_bytes_per_step": IN_BYTES,
+                    "d2h_bytes_per_step": D2H_BYTES,
+                    "api": "pipeline_unsharp (host buffers, synchronous)"},
+            "roofline": {"bound": "hbm", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": peak_kind,
+                         "alg_bytes_per_launch": ALG_BYTES,
+                         "kernel_ms": kern_ms},
+            "gpu_launches": args.steps,
+            "clocks": clk,
+        }
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline()
+        print(json.dumps(line))
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="polymage_b200",
+                    choices=["polymage_b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -276,6 +276,11 @@ class ExprCtx(object):
         return self.expr(e, {})
 
 
+def _opt(pipeline, name, default=None):
+    from .tiling import _option
+    return _option(pipeline, name, default)
+
+
 def _vn(v):
     return "v_" + re.sub(r'[^A-Za-z0-9_]', '_', v.name)
 
@@ -874,6 +879,9 @@ class StencilGen(object):
 
     def __init__(self, pg, group):
         self.pg = pg
+        self.fast = False
+        self.inside = False
+        self.has_inside = False
         self.g = group
         self.plan = group.plan
         self.k = "pm_%s_g%d" % (pg.pname, group.level_time)
@@ -1048,10 +1056,77 @@ class StencilGen(object):
                       "r_%s_hi%d, pm_imax(ea, eb)); }" % (
                           a, b, nm, d, nm, d, nm, d, nm, d))
                 w.close()
+            if n.role in ('global', 'inline'):
+                continue          # footprint only: used by the fast check
             for d in range(nd):
                 w("r_%s_lo%d = pm_imax(r_%s_lo%d, d_%s_lo%d); r_%s_hi%d = "
                   "pm_imin(r_%s_hi%d, d_%s_hi%d);" % (nm, d, nm, d, fnm, d,
                                                       nm, d, nm, d, fnm, d))
+        # Interior tile: no region was clamped by a domain, so every read of
+        # every point of every region is inside its buffer and stages can be
+        # evaluated without guards (select-based cases, register blocking).
+        conds = []
+        for n in plan.nodes:
+            nm = self.node_name(n)
+            fnm = pg.fn(n.func)
+            if n.role == 'global':
+                for d in range(n.ndims):
+                    if all(fns[d].kind != 'full' for _, fns in n.uses):
+                        conds.append("r_%s_lo%d >= d_%s_lo%d && r_%s_hi%d <= "
+                                     "d_%s_hi%d" % (nm, d, fnm, d, nm, d,
+                                                    fnm, d))
+                continue
+            if n.role == 'inline':
+                continue
+            for d, e in enumerate(self.loop_ext(n)):
+                conds.append("r_%s_hi%d - r_%s_lo%d + 1 == %d" % (nm, d, nm,
+                                                                  d, e))
+        w("const bool pm_fast = %s;" % (" && ".join(conds) or "true"))
+        w("(void)pm_fast;")
+        # Inside tile: every stage has one box-shaped Case that holds on its
+        # whole region here, so conditions can be dropped altogether.
+        inside = self.inside_conds()
+        self.has_inside = inside is not None
+        if inside is not None:
+            w("const bool pm_inside = pm_fast && %s;" % (
+                " && ".join(inside) or "true"))
+
+    def inside_conds(self):
+        """Tile-level conditions under which every stage's Case holds on the
+        stage's whole region; None when some stage is piecewise or its
+        condition is not a box."""
+        pg = self.pg
+        plan = self.plan
+        ctx = self.ctx
+        out = []
+        for f in plan.funcs:
+            parts = body_parts(f)
+            if len(parts) == 1 and parts[0][0] is None:
+                continue
+            if len(parts) != 1:
+                return None
+            boxes = part_boxes(f)
+            if len(boxes) != 1 or not boxes[0][0].exact:
+                return None
+            n = plan.node_of.get(f)
+            if n is None:
+                continue              # never evaluated in this group
+            box = boxes[0][0]
+            nm = self.node_name(n)
+            for d, v in enumerate(f.variables):
+                for e in box.lo[v]:
+                    out.append("r_%s_lo%d >= %s" % (nm, d, ctx.expr(e, {})))
+                for e in box.hi[v]:
+                    out.append("r_%s_hi%d <= %s" % (nm, d, ctx.expr(e, {})))
+        return out
+
+    def loop_ext(self, n):
+        """Static extents of the box a node is computed (or staged) over."""
+        if n.role == 'out' and not n.in_smem:
+            na = self.plan.anchor.ndims
+            return [min(e, t) for e, t in zip(n.ext,
+                                              self.plan.tile[na - n.ndims:])]
+        return list(n.ext)
 
     def decl_smem_origin(self, n):
         """Smem layout of a node: dense [E0][E1]..[E_inner] (inner padded
@@ -1147,6 +1222,27 @@ class StencilGen(object):
             w("%s = (%s)(%s);" % (target, ctype(f.typ), e))
             if written_flag:
                 w("%s = true;" % written_flag)
+            return
+        if self.inside:
+            # the single Case holds on the whole region of this tile
+            e = ctx.expr(parts[0][1], bind)
+            w("%s = (%s)(%s);" % (target, ctype(f.typ), e))
+            if written_flag:
+                w("%s = true;" % written_flag)
+            return
+        if self.fast:
+            # unguarded: every case evaluated, later cases take precedence
+            T = ctype(f.typ)
+            val = "(%s)0" % T
+            cs = []
+            for cond, expr, red in parts:
+                c = ctx.cond(cond, bind) if cond is not None else "true"
+                e = ctx.expr(expr, bind)
+                cs.append(c)
+                val = "(%s ? (%s)(%s) : %s)" % (c, T, e, val)
+            w("%s = %s;" % (target, val))
+            if written_flag:
+                w("%s = %s;" % (written_flag, " || ".join(cs)))
             return
         first = True
         for cond, expr, red in reversed(parts):
@@ -1255,21 +1351,70 @@ class StencilGen(object):
         plan = self.plan
         w = pg.w
         n = plan.node_of[f]
-        nm = self.node_name(n)
-        fnm = pg.fn(f)
-        nd = n.ndims
-        comp = pg.p.func_map[f]
-        is_out = n.role == 'out'
-        pipe_out = comp.is_output
-        ext = n.ext if n.in_smem else \
-            [min(e, t) for e, t in zip(n.ext, plan.tile[plan.anchor.ndims -
-                                                        nd:])]
-        tot = 1
-        for e in ext:
-            tot *= e
+        ext = self.loop_ext(n)
         w("// stage %s (%s%s)" % (f.name, n.role,
                                   "+smem" if n.also_smem else ""))
         w.open("")
+        if 'no_fast' not in pg.p.options:
+            if self.has_inside:
+                w.open("if (pm_inside)")
+                self.fast = self.inside = True
+                self.gen_fast_loop(f, n, ext)
+                self.fast = self.inside = False
+                w.close()
+                w.open("else if (pm_fast)")
+            else:
+                w.open("if (pm_fast)")
+            self.fast = True
+            self.gen_fast_loop(f, n, ext)
+            self.fast = False
+            w.close()
+            w.open("else")
+            self.gen_guarded_loop(f, n, ext)
+            w.close()
+        else:
+            self.gen_guarded_loop(f, n, ext)
+        w.close()
+        if n.in_smem:
+            w("__syncthreads();")
+
+    def _store(self, f, n, qs, val, flag, smem_idx, gidx=None):
+        """Store one computed point: shared memory and/or HBM (owned
+        points; pipeline outputs only where some case held)."""
+        pg = self.pg
+        plan = self.plan
+        w = pg.w
+        nm = self.node_name(n)
+        fnm = pg.fn(f)
+        nd = n.ndims
+        if n.in_smem:
+            w("sm_%s[%s] = %s;" % (nm, smem_idx, val))
+        if n.role == 'out':
+            own = ""
+            if n.func is not plan.anchor and n.also_smem:
+                own = " && ".join("%s >= o_%s_lo%d && %s <= o_%s_hi%d" % (
+                    qs[d], nm, d, qs[d], nm, d) for d in range(nd))
+            cond = " && ".join(x for x in [own, flag or ""] if x)
+            idx = gidx or " + ".join(
+                ["(long long)(%s - d_%s_lo%d) * s_%s_%d" % (qs[d], fnm, d,
+                                                            fnm, d)
+                 for d in range(nd)])
+            if cond:
+                w("if (%s) b_%s[%s] = %s;" % (cond, fnm, idx, val))
+            else:
+                w("b_%s[%s] = %s;" % (fnm, idx, val))
+
+    def gen_guarded_loop(self, f, n, ext):
+        """Border tiles: one point per iteration, guarded by the region."""
+        pg = self.pg
+        plan = self.plan
+        w = pg.w
+        nm = self.node_name(n)
+        nd = n.ndims
+        comp = pg.p.func_map[f]
+        tot = 1
+        for e in ext:
+            tot *= e
         w.open("for (int i = threadIdx.x; i < %d; i += %d)" % (
             tot, plan.threads))
         self.decompose("i", ext, "j")
@@ -1283,30 +1428,100 @@ class StencilGen(object):
         bind = dict(zip(f.variables, lv))
         w("%s v = 0;" % ctype(f.typ))
         flag = None
-        if is_out and pipe_out:
+        if n.role == 'out' and comp.is_output:
             w("bool wr = false;")
             flag = "wr"
         self.emit_cases(f, bind, "v", flag)
-        if n.in_smem:
-            w("sm_%s[i] = v;" % nm)
-        if is_out:
-            own = ""
-            if n.func is not plan.anchor and n.also_smem:
-                own = " && ".join("q%d >= o_%s_lo%d && q%d <= o_%s_hi%d" % (
-                    d, nm, d, d, nm, d) for d in range(nd))
-            cond = " && ".join(x for x in [own, flag or ""] if x)
-            idx = " + ".join(
-                ["(long long)(q%d - d_%s_lo%d) * s_%s_%d" % (d, fnm, d, fnm, d)
-                 for d in range(nd)])
-            if cond:
-                w("if (%s) b_%s[%s] = v;" % (cond, fnm, idx))
-            else:
-                w("b_%s[%s] = v;" % (fnm, idx))
+        self._store(f, n, ["q%d" % d for d in range(nd)], "v", flag, "i")
         ctx.pop()
         w.close()
+
+    def gen_fast_loop(self, f, n, ext):
+        """Interior tiles: each thread computes a block of ``rb`` points
+        along the second-innermost dimension (consecutive threads take
+        consecutive innermost points, so shared-memory accesses stay
+        conflict-free and HBM accesses coalesced); reads shared by the
+        block's points are loaded once."""
+        pg = self.pg
+        plan = self.plan
+        w = pg.w
+        nm = self.node_name(n)
+        nd = n.ndims
+        comp = pg.p.func_map[f]
+        rb_max = int(_opt(pg.p, 'rblock', 4))
+        inner = ext[-1]
+        if nd >= 2:
+            outer = ext[-2]
+            K = 1
+            for k in (8, 4, 2, 1):
+                if k <= rb_max and outer % k == 0:
+                    K = k
+                    break
+        else:
+            outer, K = 1, 1
+        nblk = outer // K
+        rest = ext[:-2] if nd >= 2 else []
+        total = nblk * inner
+        for e in rest:
+            total *= e
+        strides = []
+        st = 1
+        for e in reversed(ext):
+            strides.insert(0, st)
+            st *= e
+        w.open("for (int it = threadIdx.x; it < %d; it += %d)" % (
+            total, plan.threads))
+        w("const int ji = it %% %d; int rr = it / %d;" % (inner, inner))
+        if nd >= 2:
+            w("const int jo = (rr %% %d) * %d; rr /= %d;" % (nblk, K, nblk))
+        for d in range(len(rest) - 1, -1, -1):
+            if d == 0:
+                w("const int j%d = rr;" % d)
+            else:
+                w("const int j%d = rr %% %d; rr /= %d;" % (d, rest[d],
+                                                          rest[d]))
+        base = _loop_vars(nd, "qb")
+        for d in range(nd):
+            if d == nd - 1:
+                j = "ji"
+            elif d == nd - 2:
+                j = "jo"
+            else:
+                j = "j%d" % d
+            w("const int qb%d = r_%s_lo%d + %s;" % (d, nm, d, j))
+        w("const int ib = %s;" % " + ".join(
+            "(qb%d - r_%s_lo%d) * %d" % (d, nm, d, strides[d])
+            for d in range(nd)))
+        fnm = pg.fn(f)
+        if n.role == 'out':
+            w("const long long gb = %s;" % " + ".join(
+                "(long long)(qb%d - d_%s_lo%d) * s_%s_%d" % (d, fnm, d, fnm, d)
+                for d in range(nd)))
+        ctx = self.ctx
+        ctx.push()
+        flagged = n.role == 'out' and comp.is_output
+        for k in range(K):
+            pt = list(base)
+            qs = ["qb%d" % d for d in range(nd)]
+            if nd >= 2 and k:
+                pt[nd - 2] = base[nd - 2] + k
+                qs[nd - 2] = "(qb%d + %d)" % (nd - 2, k)
+            bind = dict(zip(f.variables, pt))
+            v = "v%d" % k
+            w("%s %s = 0;" % (ctype(f.typ), v))
+            flag = None
+            if flagged:
+                flag = "wr%d" % k
+                w("bool %s = false;" % flag)
+            self.emit_cases(f, bind, v, flag)
+            idx = "ib" if k == 0 else "ib + %d" % (k * strides[nd - 2])
+            gidx = None
+            if n.role == 'out':
+                gidx = "gb" if k == 0 else "gb + %d * s_%s_%d" % (
+                    k, fnm, nd - 2)
+            self._store(f, n, qs, v, flag, idx, gidx)
+        ctx.pop()
         w.close()
-        if n.in_smem:
-            w("__syncthreads();")
 
     # ---- launcher -------------------------------------------------------------
     def gen_launcher(self):

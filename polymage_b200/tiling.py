@@ -142,12 +142,13 @@ def expr_cost(e):
 
 
 def func_cost(f):
+    """Recompute cost of a stage at one point: its expressions (the Case
+    conditions are cheap comparisons shared by neighbouring points and are
+    not counted)."""
     from .pipe import body_parts
     total = 0
     for cond, expr, red in body_parts(f):
         total += expr_cost(expr)
-        if cond is not None:
-            total += expr_cost(cond)
     return total
 
 
@@ -459,10 +460,23 @@ def plan_stencil(pipeline, comps):
         plan.ext_role[x] = 'stage' if want else 'global'
         if want:
             mk(x, 'stage')
+    # externals read straight from HBM get a footprint node too (never
+    # materialized): the kernel uses it to prove that an interior tile's
+    # reads stay inside the buffer before taking its unguarded fast path
+    for x in externals:
+        if plan.ext_role[x] == 'global':
+            mk(x, 'global')
+    # stages computed in registers get a footprint node as well: the kernel
+    # checks their Case conditions against it to drop them on tiles where
+    # they hold everywhere
+    for f in reversed(funcs):
+        if role[f] == 'inline' and uses[f]:
+            mk(f, 'inline')
 
     # attach uses as (node, IndexFn list)
     for n in nodes:
-        src = ext_uses[n.func] if n.role == 'stage' else uses[n.func]
+        src = ext_uses[n.func] if n.role in ('stage', 'global') \
+            else uses[n.func]
         for m, args in src:
             if m not in node_of:
                 raise PlanError("internal: consumer %s not materialized"
@@ -492,7 +506,8 @@ def plan_stencil(pipeline, comps):
     steps = [f for f in funcs if role[f] in ('out', 'smem')]
     plan.steps = steps
     for n in nodes:
-        n.step = 0 if n.role == 'stage' else steps.index(n.func) + 1
+        n.step = 0 if n.role in ('stage', 'global', 'inline') else \
+            steps.index(n.func) + 1
     for n in nodes:
         last = n.step
         for m, _ in n.uses:

@@ -12,5 +12,5 @@ def harris(tile=(32, 128)):
 
 
 @functools.lru_cache(maxsize=None)
-def unsharp(tile=(16, 128)):
+def unsharp(tile=(32, 128)):
     return build_unsharp(tile_sizes=tile).build()
