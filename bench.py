@@ -36,7 +36,6 @@ sys.path.insert(0, ROOT)
 
 R = C = 4096
 THRESHOLD, WEIGHT = 0.001, 3.0
-TILE = (32, 128)
 IN_BYTES = 3 * (R + 4) * (C + 4) * 4
 OUT_BYTES = 3 * R * C * 4
 ALG_BYTES = IN_BYTES + OUT_BYTES          # compulsory bytes per step
@@ -209,7 +208,8 @@ def run(args):
     from polymage_b200.apps.unsharp_mask import build_unsharp
     import oracle.unsharp as OU
 
-    cp = build_unsharp(tile_sizes=TILE).build()
+    from polymage_b200.apps import catalog
+    cp = build_unsharp(**catalog.UNSHARP).build()
     kernel = cp.module.meta['groups'][0]['kernel']
     prm = {'R': R, 'C': C, 'threshold': THRESHOLD, 'weight': WEIGHT}
     host_in = OU.make_input(R, C, seed=0)
@@ -289,7 +289,9 @@ def run(args):
             "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32",
             "data": "synthetic: U[0,1) seed 0, 2-px zero ghost zone",
-            "config": {"workload": WORKLOAD, "tile": list(TILE),
+            "config": {"workload": WORKLOAD,
+                       "tile": list(catalog.UNSHARP["tile_sizes"]),
+                       "options": list(catalog.UNSHARP["options"]),
                        "kernel": kernel,
                        "l2": "inputs larger than L2 (201.7 MB in + 201.3 MB "
                              "out per step vs 126 MB L2)",

@@ -1038,23 +1038,25 @@ class StencilGen(object):
                 for d in range(nd):
                     w("int r_%s_lo%d = %s, r_%s_hi%d = -%s;" % (nm, d, big,
                                                                 nm, d, big))
-            for m, fns in n.uses:
+            for m, per_dim in self.distinct_uses(n):
                 mn = self.node_name(m)
                 w.open("if (!(%s))" % self.empty_expr(m))
-                for d, fn in enumerate(fns):
-                    if fn.kind == 'mono':
-                        a = ctx.expr(fn.expr, {fn.var: "r_%s_lo%d" % (
-                            mn, fn.cdim)})
-                        b = ctx.expr(fn.expr, {fn.var: "r_%s_hi%d" % (
-                            mn, fn.cdim)})
-                    elif fn.kind == 'const':
-                        a = b = ctx.expr(fn.expr, {})
-                    else:
-                        a, b = "d_%s_lo%d" % (fnm, d), "d_%s_hi%d" % (fnm, d)
-                    w("{ const int ea = %s, eb = %s; r_%s_lo%d = pm_imin("
-                      "r_%s_lo%d, pm_imin(ea, eb)); r_%s_hi%d = pm_imax("
-                      "r_%s_hi%d, pm_imax(ea, eb)); }" % (
-                          a, b, nm, d, nm, d, nm, d, nm, d))
+                for d, fns in enumerate(per_dim):
+                    for fn in fns:
+                        if fn.kind == 'mono':
+                            a = ctx.expr(fn.expr, {fn.var: "r_%s_lo%d" % (
+                                mn, fn.cdim)})
+                            b = ctx.expr(fn.expr, {fn.var: "r_%s_hi%d" % (
+                                mn, fn.cdim)})
+                        elif fn.kind == 'const':
+                            a = b = ctx.expr(fn.expr, {})
+                        else:
+                            a, b = ("d_%s_lo%d" % (fnm, d),
+                                    "d_%s_hi%d" % (fnm, d))
+                        w("{ const int ea = %s, eb = %s; r_%s_lo%d = "
+                          "pm_imin(r_%s_lo%d, pm_imin(ea, eb)); r_%s_hi%d = "
+                          "pm_imax(r_%s_hi%d, pm_imax(ea, eb)); }" % (
+                              a, b, nm, d, nm, d, nm, d, nm, d))
                 w.close()
             if n.role in ('global', 'inline'):
                 continue          # footprint only: used by the fast check
@@ -1115,9 +1117,55 @@ class StencilGen(object):
             nm = self.node_name(n)
             for d, v in enumerate(f.variables):
                 for e in box.lo[v]:
-                    out.append("r_%s_lo%d >= %s" % (nm, d, ctx.expr(e, {})))
+                    c = "r_%s_lo%d >= %s" % (nm, d, ctx.expr(e, {}))
+                    if c not in out:
+                        out.append(c)
                 for e in box.hi[v]:
-                    out.append("r_%s_hi%d <= %s" % (nm, d, ctx.expr(e, {})))
+                    c = "r_%s_hi%d <= %s" % (nm, d, ctx.expr(e, {}))
+                    if c not in out:
+                        out.append(c)
+        return out
+
+    def distinct_uses(self, n):
+        """Uses of a node grouped by consumer, with per-dimension index
+        functions deduplicated; of affine functions ``a*v + c`` differing
+        only in ``c`` just the smallest and largest ``c`` are kept (the
+        others cannot extend the union)."""
+        from .expression import affine_form
+        out = []
+        for m in [u[0] for u in n.uses]:
+            if any(m is o[0] for o in out):
+                continue
+            per_dim = []
+            for d in range(n.ndims):
+                fns = [fns_[d] for mm, fns_ in n.uses if mm is m]
+                keep = []
+                seen = set()
+                groups = {}
+                for fn in fns:
+                    k = fn.key()
+                    if k in seen:
+                        continue
+                    seen.add(k)
+                    f = affine_form(fn.expr) if fn.kind == 'mono' else None
+                    if f is not None and all(not isinstance(v, C.Parameter)
+                                             for v in f[0]):
+                        gk = tuple(sorted((v.name, c) for v, c in
+                                          f[0].items()))
+                        lo, hi = groups.get(gk, (None, None))
+                        if lo is None or f[1] < lo[1]:
+                            lo = (fn, f[1])
+                        if hi is None or f[1] > hi[1]:
+                            hi = (fn, f[1])
+                        groups[gk] = (lo, hi)
+                    else:
+                        keep.append(fn)
+                for lo, hi in groups.values():
+                    keep.append(lo[0])
+                    if hi[0] is not lo[0]:
+                        keep.append(hi[0])
+                per_dim.append(keep)
+            out.append((m, per_dim))
         return out
 
     def loop_ext(self, n):

@@ -780,7 +780,10 @@ class Stencil(AbstractExpression):
     weights dropped and unit weights unmultiplied, in row-major kernel
     order (sandbox/constructs.py:544-687)."""
 
-    def __init__(self, input_fn, iteration_vars, kernel, origin=None):
+    def __init__(self, input_fn, iteration_vars, kernel, origin=None,
+                 _origin=None):
+        if origin is None:
+            origin = _origin
         if not isinstance(input_fn, Function):
             raise TypeError("Expected %s to be of type Function" % input_fn)
         for v in iteration_vars:

@@ -661,8 +661,13 @@ def _static_extents(plan, env):
     for n in plan.nodes:
         a, b = exts[0][n.func], exts[1][n.func]
         if a != b:
-            raise PlanError("inconsistent scaling: footprint of %s grows "
-                            "with the tile origin" % n.name)
+            if n.role == 'stage':
+                # an input read at inconsistent scales is not staged
+                n.role = 'global'
+                plan.ext_role[n.func] = 'global'
+            elif n.role not in ('global', 'inline'):
+                raise PlanError("inconsistent scaling: footprint of %s "
+                                "grows with the tile origin" % n.name)
         if n.func is plan.anchor or n.role == 'out' and not n.also_smem:
             n.ext = [min(x, t) for x, t in
                      zip(a, plan.tile[plan.anchor.ndims - n.ndims:])]
@@ -706,6 +711,9 @@ def _alignment(plan, env):
                     n.align[d] = m.align[fn.cdim]
                     n.scale[d] = s
                 elif n.align[d] == m.align[fn.cdim] and n.scale[d] != s:
+                    if n.role in ('global', 'inline'):
+                        n.scale[d] = None      # read at several scales
+                        continue
                     raise PlanError("inconsistent scaling of %s" % n.name)
 
 

@@ -1,0 +1,99 @@
+"""Compiler passes and plans (no GPU): grouping, materialization,
+static extents vs exhaustive region simulation, validation and codegen."""
+
+import numpy as np
+import pytest
+
+from polymage_b200.constructs import *   # noqa: F401,F403
+from polymage_b200.compiler import buildPipeline
+from polymage_b200.apps.harris import build_harris
+from polymage_b200.apps.unsharp_mask import build_unsharp
+from polymage_b200.tiling import infer_regions, PlanError
+
+
+def test_harris_single_group_like_reference():
+    p = build_harris(tile_sizes=(32, 128))
+    assert len(p.groups) == 1           # all 11 stages, group_size 11
+    plan = p.groups[0].plan
+    mat = sorted(f.name for f in plan.steps)
+    assert mat == ['Ix', 'Iy', 'harris']
+    staged = [n.name for n in plan.nodes if n.role == 'stage']
+    assert staged == ['img']
+    ext = dict((n.name, n.ext) for n in plan.nodes)
+    assert ext['Ix'] == [34, 130] and ext['img'] == [36, 132]
+
+
+def test_unsharp_plan():
+    p = build_unsharp(tile_sizes=(32, 128))
+    assert len(p.groups) == 1
+    plan = p.groups[0].plan
+    assert [f.name for f in plan.steps] == ['blurx', 'mask']
+    ext = dict((n.name, n.ext) for n in plan.nodes)
+    assert ext['blurx'] == [1, 32, 132] and ext['img'] == [1, 36, 132]
+    assert plan.smem_bytes <= 48 * 1024
+
+
+@pytest.mark.parametrize("build", [build_harris, build_unsharp])
+def test_static_extents_bound_every_tile(build):
+    """Run region inference for every tile of a small image and check each
+    region fits the static (shared-memory) extents."""
+    p = build(tile_sizes=(16, 32))
+    plan = p.groups[0].plan
+    env = p.int_env()
+    for k in list(env):
+        env[k] = 61 if k.name in ('R', 'C') else env[k]
+    anchor = plan.anchor
+    dom = [(int(__import__('polymage_b200.evaluate', fromlist=['x'])
+                .eval_int(d.lowerBound, env)),
+            int(__import__('polymage_b200.evaluate', fromlist=['x'])
+                .eval_int(d.upperBound, env))) for d in anchor.domain]
+    T = plan.tile
+    starts = [range(lo, hi + 1, t) for (lo, hi), t in zip(dom, T)]
+    import itertools
+    for origin in itertools.product(*starts):
+        box = [(o, min(o + t - 1, hi)) for o, t, (lo, hi) in
+               zip(origin, T, dom)]
+        regs = infer_regions(plan, box, env)
+        for n in plan.nodes:
+            if n.role in ('global', 'inline'):
+                continue
+            lo, hi = regs[n.func]
+            for d in range(n.ndims):
+                assert int(hi[d]) - int(lo[d]) + 1 <= n.ext[d]
+
+
+def test_out_of_domain_reference_rejected():
+    R = Parameter(Int, "R")
+    x = Variable(Int, "x")
+    img = Image(Float, "img", [R])
+    f = Function(([x], [Interval(Int, 0, R - 1)]), Float, "f")
+    f.defn = [img(x + 1)]
+    with pytest.raises(TypeError):
+        buildPipeline([f], param_estimates=[(R, 100)])
+
+
+def test_inconsistent_scaling_splits_group():
+    """A stage read both at x and x/2 cannot be tiled with the reader."""
+    R = Parameter(Int, "R")
+    x = Variable(Int, "x")
+    img = Image(Float, "img", [R])
+    a = Function(([x], [Interval(Int, 0, R - 1)]), Float, "a")
+    a.defn = [img(x) * 2.0]
+    b = Function(([x], [Interval(Int, 0, R - 1)]), Float, "b")
+    b.defn = [a(x) + a(x / 2)]
+    p = buildPipeline([b], param_estimates=[(R, 4096)], group_size=5)
+    assert len(p.groups) == 2
+
+
+def test_generated_source_has_tma_and_no_multicast():
+    p = build_unsharp(tile_sizes=(32, 128))
+    src = p.generate_code().source
+    assert 'pm_tma_load_3d' in src
+    assert 'multicast' not in src
+    assert '__launch_bounds__' in src
+
+
+def test_grouping_respects_group_size():
+    p = build_harris(tile_sizes=(32, 128), group_size=3)
+    assert all(len(g.comps) <= 3 for g in p.groups)
+    assert len(p.groups) > 1

@@ -1,0 +1,46 @@
+"""The oracle's restatements pinned to the reference's own generated C++
+(golden fixtures in tests/golden, made by tests/golden/make_golden.py)."""
+
+import os
+
+import numpy as np
+
+import oracle.harris as OH
+import oracle.unsharp as OU
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def test_harris_matches_reference_cpp():
+    g = np.load(os.path.join(GOLD, "harris.npz"))
+    ours = OH.harris(g["img"])
+    ref = g["out"].astype(np.float64)
+    # refHarris computes in float32: compare relative to the output scale
+    assert np.abs(ours - ref).max() / np.abs(ref).max() < 1e-6
+    # refHarris zero-fills; both leave the 2-pixel border at 0
+    H, W = ref.shape
+    mask = np.ones_like(ref, dtype=bool)
+    mask[2:H - 1, 2:W - 1] = False
+    assert np.all(ref[mask] == 0) and np.all(ours[mask] == 0)
+
+
+def test_unsharp_matches_reference_cpp_on_defined_region():
+    g = np.load(os.path.join(GOLD, "unsharp.npz"))
+    u8 = g["img"]
+    thr, w = float(g["threshold"]), float(g["weight"])
+    planar = np.moveaxis(u8.astype(np.float32) / np.float32(255.0), 2, 0)
+    ours = OU.unsharp(planar, thr, w)
+    ref = np.moveaxis(g["out"], 2, 0).astype(np.float64)
+    R, C = ref.shape[1:]
+    xs, ys = OU.defined_region(R, C)
+    m = OU.margin(planar, thr)[:, xs, ys] > 1e-6
+    d = np.abs(ours[:, xs, ys] - ref[:, xs, ys])
+    assert d[m].max() < 1e-5
+
+
+def test_unsharp_convention_outside_defined_region():
+    """Columns whose blur reaches uncomputed blurx points use 0 there."""
+    img = OU.make_input(10, 12, seed=4)
+    out = OU.unsharp(img, 0.001, 3.0)
+    assert out.shape == (3, 10, 12)
+    assert np.all(out[:, 9, :] == 0) and np.all(out[:, :, 11] == 0)
