@@ -5,13 +5,29 @@ import functools
 
 from .harris import build_harris
 from .unsharp_mask import build_unsharp
+from .campipe import build_campipe
 
 HARRIS = dict(tile_sizes=(32, 64), options=('rblock=4',))
 UNSHARP = dict(tile_sizes=(32, 128), options=('rblock=8',))
+CAMPIPE = dict(tile_sizes=(32, 128), group_size=5, options=('rblock=4',))
+
+_BUILDERS = {
+    "harris": (build_harris, HARRIS),
+    "unsharp": (build_unsharp, UNSHARP),
+    "campipe": (build_campipe, CAMPIPE),
+}
+
+_cache = {}
 
 
 def default_builds():
-    return [
-        ("harris", functools.partial(build_harris, **HARRIS)),
-        ("unsharp", functools.partial(build_unsharp, **UNSHARP)),
-    ]
+    return [(name, functools.partial(b, **kw))
+            for name, (b, kw) in _BUILDERS.items()]
+
+
+def build(name):
+    """The compiled default build of a shipped pipeline (cached)."""
+    if name not in _cache:
+        b, kw = _BUILDERS[name]
+        _cache[name] = b(**kw).build()
+    return _cache[name]

@@ -2051,6 +2051,10 @@ class ConstGen(object):
         self.reads = reads
         pg.meta['groups'].append({'kernel': None, 'kind': 'const',
                                   'stages': [f.name]})
+        pg.meta.setdefault('const', {})[f.name] = {
+            'symbol': "pm_const_%s_%s" % (pg.pname, fnm),
+            'params': [q.name for q in pg.params],
+            'reads': [o.name for o in reads]}
         # ---- host C++ tabulation (compiled by g++ with the reference's
         # flags) ----
         hparams = ", ".join(["%s %s" % (pg.ptype(q), pg.pmap[q])

@@ -624,16 +624,31 @@ def infer_regions(plan, anchor_box, env, clamp=True, tile_first=None):
 
 
 def _static_extents(plan, env):
+    # period of every node's region in the tile origin: the lcm, over the
+    # chains of uses from the anchor, of the product of the divisors met
+    per = {}
+    capped = False
     divs = []
     for n in plan.nodes:
+        p = 1
         for m, fns in n.uses:
+            q = per.get(m.func, 1)
             for fn in fns:
                 if fn.kind == 'mono':
-                    divs += divisors_in(fn.expr)
-    prod = 1
-    for q in divs:
-        prod = min(prod * q, MAX_PERIOD)
-    period = prod
+                    for dv in divisors_in(fn.expr):
+                        q *= dv
+                        divs.append(dv)
+            p = p * q // math.gcd(p, q)
+        if p > MAX_PERIOD:
+            capped = True
+            p = MAX_PERIOD
+        per[n.func] = p
+    period = 1
+    for p in per.values():
+        period = period * p // math.gcd(period, p)
+        if period > MAX_PERIOD:
+            capped = True
+            period = MAX_PERIOD
     plan.period = period
     exts = []
     for base in (period * (1 << 22), period * (1 << 23) + period * 7):
@@ -673,7 +688,7 @@ def _static_extents(plan, env):
                      zip(a, plan.tile[plan.anchor.ndims - n.ndims:])]
         else:
             n.ext = a
-        if period == MAX_PERIOD and len(divs) > 1:
+        if capped:
             n.ext = [x + 2 for x in n.ext]
 
 
