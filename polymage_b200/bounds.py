@@ -57,31 +57,69 @@ class PartBox(object):
         return out
 
 
+def _split_linear(e, variables):
+    """(coeffs of loop variables, remainder) of ``e`` when ``e`` is a sum
+    of integer multiples of loop variables and variable-free terms (which
+    may be any parameter expression, divisions included); None otherwise."""
+    e = Value.numericToValue(e)
+    vs = [v for v in e.collect(C.Variable) if not isinstance(v, C.Parameter)]
+    if not vs:
+        return {}, e
+    if isinstance(e, C.Variable):
+        if any(e is v for v in variables):
+            return {e: 1}, Value(0, C.Int)
+        return None
+    from .expr_ast import AbstractBinaryOpNode, AbstractUnaryOpNode
+    if isinstance(e, AbstractUnaryOpNode):
+        r = _split_linear(e.child, variables)
+        if r is None:
+            return None
+        if e.op == '-':
+            return dict((k, -c) for k, c in r[0].items()), 0 - r[1]
+        return r
+    if isinstance(e, AbstractBinaryOpNode):
+        if e.op in ('+', '-'):
+            a = _split_linear(e.left, variables)
+            b = _split_linear(e.right, variables)
+            if a is None or b is None:
+                return None
+            s = 1 if e.op == '+' else -1
+            co = dict(a[0])
+            for k, c in b[0].items():
+                co[k] = co.get(k, 0) + s * c
+            return co, (a[1] + b[1]) if s == 1 else (a[1] - b[1])
+        if e.op == '*':
+            for lin, k in ((e.left, e.right), (e.right, e.left)):
+                k = Value.numericToValue(k)
+                if isinstance(k, Value) and isinstance(k.value, int):
+                    r = _split_linear(lin, variables)
+                    if r is None:
+                        return None
+                    return (dict((v, c * k.value) for v, c in r[0].items()),
+                            r[1] * k.value)
+        return None
+    return None
+
+
 def _var_bound(cmp_cond, variables):
     """Translate ``a*v + rest (op) 0`` with a = +-1 into bounds on v.
     Returns ('lo'|'hi'|'eq', v, expr) items, or None if not of that form."""
-    lf = affine_form(cmp_cond.lhs)
-    rf = affine_form(cmp_cond.rhs)
+    lf = _split_linear(cmp_cond.lhs, variables)
+    rf = _split_linear(cmp_cond.rhs, variables)
     if lf is None or rf is None:
         return None
     coeffs = dict(lf[0])
     for k, c in rf[0].items():
         coeffs[k] = coeffs.get(k, 0) - c
-    const = lf[1] - rf[1]
-    vs = [k for k, c in coeffs.items() if c != 0 and
-          not isinstance(k, C.Parameter)]
-    if len(vs) != 1 or vs[0] not in variables:
+    vs = [k for k, c in coeffs.items() if c != 0]
+    if len(vs) != 1 or not any(vs[0] is v for v in variables):
         return None
     v = vs[0]
     a = coeffs[v]
     if a not in (1, -1):
         return None
-    # rest = sum(param terms) + const ; condition: a*v + rest op 0
-    rest = Value(const, C.Int)
-    for k, c in coeffs.items():
-        if k is v or c == 0:
-            continue
-        rest = rest + c * k
+    # condition: a*v + rest op 0
+    rest = lf[1] - rf[1]
     # v op' (-rest)/a
     op = cmp_cond.conditional
     if a == -1:

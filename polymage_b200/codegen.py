@@ -360,7 +360,7 @@ class PipelineGen(object):
                   "(d_%s_hi%d - d_%s_lo%d + 1);" % (n, d, n, d + 1, n, d + 1,
                                                     n, d + 1))
 
-    def gindex(self, f, args, ctx, clamp_dd=True):
+    def gindex(self, f, args, ctx, clamp_dd=True, clamp_all=False):
         """Linear index into a dense array of ``f`` at index ASTs ``args``;
         data-dependent components are clamped into the domain."""
         n = self.fn(f)
@@ -368,7 +368,7 @@ class PipelineGen(object):
         nd = len(args)
         for d, a in enumerate(args):
             s = ctx.index(a)
-            if clamp_dd and is_data_dependent(a):
+            if clamp_all or (clamp_dd and is_data_dependent(a)):
                 s = "pm_clampi(%s, d_%s_lo%d, d_%s_hi%d)" % (s, n, d, n, d)
             if d == nd - 1:
                 terms.append("(long long)(%s - d_%s_lo%d)" % (s, n, d))
@@ -880,6 +880,7 @@ class StencilGen(object):
     def __init__(self, pg, group):
         self.pg = pg
         self.fast = False
+        self.clamp = False
         self.inside = False
         self.has_inside = False
         self.g = group
@@ -1001,9 +1002,10 @@ class StencilGen(object):
         w.close()
         w("")
 
-    def empty_expr(self, n):
+    def empty_expr(self, n, kind="r"):
         nm = self.node_name(n)
-        return " || ".join("r_%s_lo%d > r_%s_hi%d" % (nm, d, nm, d)
+        return " || ".join("%s_%s_lo%d > %s_%s_hi%d" % (kind, nm, d, kind,
+                                                        nm, d)
                            for d in range(n.ndims))
 
     def gen_regions(self):
@@ -1022,6 +1024,7 @@ class StencilGen(object):
                     w("const int r_%s_lo%d = pm_imax(a_lo%d, d_%s_lo%d), "
                       "r_%s_hi%d = pm_imin(a_hi%d, d_%s_hi%d);" % (
                           nm, d, d, fnm, d, nm, d, d, fnm, d))
+                self.effective_bounds(n)
                 continue
             if n.role == 'out':
                 owner = " && ".join("t%d == 0" % kk
@@ -1040,13 +1043,13 @@ class StencilGen(object):
                                                                 nm, d, big))
             for m, per_dim in self.distinct_uses(n):
                 mn = self.node_name(m)
-                w.open("if (!(%s))" % self.empty_expr(m))
+                w.open("if (!(%s))" % self.empty_expr(m, "e"))
                 for d, fns in enumerate(per_dim):
                     for fn in fns:
                         if fn.kind == 'mono':
-                            a = ctx.expr(fn.expr, {fn.var: "r_%s_lo%d" % (
+                            a = ctx.expr(fn.expr, {fn.var: "e_%s_lo%d" % (
                                 mn, fn.cdim)})
-                            b = ctx.expr(fn.expr, {fn.var: "r_%s_hi%d" % (
+                            b = ctx.expr(fn.expr, {fn.var: "e_%s_hi%d" % (
                                 mn, fn.cdim)})
                         elif fn.kind == 'const':
                             a = b = ctx.expr(fn.expr, {})
@@ -1058,15 +1061,17 @@ class StencilGen(object):
                           "pm_imax(r_%s_hi%d, pm_imax(ea, eb)); }" % (
                               a, b, nm, d, nm, d, nm, d, nm, d))
                 w.close()
-            if n.role in ('global', 'inline'):
-                continue          # footprint only: used by the fast check
-            for d in range(nd):
-                w("r_%s_lo%d = pm_imax(r_%s_lo%d, d_%s_lo%d); r_%s_hi%d = "
-                  "pm_imin(r_%s_hi%d, d_%s_hi%d);" % (nm, d, nm, d, fnm, d,
-                                                      nm, d, nm, d, fnm, d))
-        # Interior tile: no region was clamped by a domain, so every read of
-        # every point of every region is inside its buffer and stages can be
-        # evaluated without guards (select-based cases, register blocking).
+            if n.role not in ('global', 'inline'):
+                # footprint-only nodes stay unclamped (used by pm_inside)
+                for d in range(nd):
+                    w("r_%s_lo%d = pm_imax(r_%s_lo%d, d_%s_lo%d); r_%s_hi%d ="
+                      " pm_imin(r_%s_hi%d, d_%s_hi%d);" % (
+                          nm, d, nm, d, fnm, d, nm, d, nm, d, fnm, d))
+            self.effective_bounds(n)
+        # Interior tile: every region is its full static box (nothing was
+        # clamped), HBM reads stay in their buffers, and every stage's single
+        # box-shaped Case holds on its whole region, so the stages can be
+        # evaluated without conditions, guards or clamped reads.
         conds = []
         for n in plan.nodes:
             nm = self.node_name(n)
@@ -1083,15 +1088,29 @@ class StencilGen(object):
             for d, e in enumerate(self.loop_ext(n)):
                 conds.append("r_%s_hi%d - r_%s_lo%d + 1 == %d" % (nm, d, nm,
                                                                   d, e))
-        w("const bool pm_fast = %s;" % (" && ".join(conds) or "true"))
-        w("(void)pm_fast;")
-        # Inside tile: every stage has one box-shaped Case that holds on its
-        # whole region here, so conditions can be dropped altogether.
         inside = self.inside_conds()
-        self.has_inside = inside is not None
-        if inside is not None:
-            w("const bool pm_inside = pm_fast && %s;" % (
-                " && ".join(inside) or "true"))
+        self.has_inside = inside is not None and \
+            'no_inside' not in pg.p.options
+        if self.has_inside:
+            w("const bool pm_inside = %s;" % (
+                " && ".join(conds + inside) or "true"))
+
+    def effective_bounds(self, n):
+        """Bounds of the points of a node that read their producers: the
+        region intersected with the node's Case box."""
+        w = self.pg.w
+        nm = self.node_name(n)
+        cb = getattr(n, 'case_box', None)
+        for d in range(n.ndims):
+            lo = "r_%s_lo%d" % (nm, d)
+            hi = "r_%s_hi%d" % (nm, d)
+            if cb:
+                for e in cb[d][0]:
+                    lo = "pm_imax(%s, %s)" % (lo, self.ctx.expr(e, {}))
+                for e in cb[d][1]:
+                    hi = "pm_imin(%s, %s)" % (hi, self.ctx.expr(e, {}))
+            w("const int e_%s_lo%d = %s, e_%s_hi%d = %s;" % (nm, d, lo, nm,
+                                                             d, hi))
 
     def inside_conds(self):
         """Tile-level conditions under which every stage's Case holds on the
@@ -1236,9 +1255,14 @@ class StencilGen(object):
         node = plan.node_of.get(f)
         t = ctx.temp()
         if node is not None and node.in_smem:
+            idx = self.smem_index(node, args)
+            if self.clamp:
+                size = 1
+                for e in node._sm_ext:
+                    size *= e
+                idx = "pm_clampi(%s, 0, %d)" % (idx, size - 1)
             w("const %s %s = sm_%s[%s];" % (ctype(f.typ), t,
-                                            self.node_name(node),
-                                            self.smem_index(node, args)))
+                                            self.node_name(node), idx))
         elif f in plan.role and plan.role[f] == 'inline':
             self.emit_inline(f, args, t)
         elif f in plan.role:
@@ -1246,7 +1270,8 @@ class StencilGen(object):
                                f.name)
         else:
             w("const %s %s = __ldg(b_%s + (%s));" % (
-                ctype(f.typ), t, pg.fn(f), pg.gindex(f, args, ctx)))
+                ctype(f.typ), t, pg.fn(f),
+                pg.gindex(f, args, ctx, clamp_all=self.clamp)))
         ctx.define(key, t)
         return t
 
@@ -1403,25 +1428,23 @@ class StencilGen(object):
         w("// stage %s (%s%s)" % (f.name, n.role,
                                   "+smem" if n.also_smem else ""))
         w.open("")
-        if 'no_fast' not in pg.p.options:
+        if 'guarded' in pg.p.options:
+            self.gen_guarded_loop(f, n, ext)
+        else:
             if self.has_inside:
                 w.open("if (pm_inside)")
                 self.fast = self.inside = True
                 self.gen_fast_loop(f, n, ext)
                 self.fast = self.inside = False
                 w.close()
-                w.open("else if (pm_fast)")
-            else:
-                w.open("if (pm_fast)")
-            self.fast = True
+                w.open("else")
+            # every point of the static box, select-based cases, clamped
+            # reads: valid on any tile
+            self.fast = self.clamp = True
             self.gen_fast_loop(f, n, ext)
-            self.fast = False
-            w.close()
-            w.open("else")
-            self.gen_guarded_loop(f, n, ext)
-            w.close()
-        else:
-            self.gen_guarded_loop(f, n, ext)
+            self.fast = self.clamp = False
+            if self.has_inside:
+                w.close()
         w.close()
         if n.in_smem:
             w("__syncthreads();")
@@ -1441,6 +1464,9 @@ class StencilGen(object):
             own = ""
             if n.func is not plan.anchor and n.also_smem:
                 own = " && ".join("%s >= o_%s_lo%d && %s <= o_%s_hi%d" % (
+                    qs[d], nm, d, qs[d], nm, d) for d in range(nd))
+            elif self.clamp:
+                own = " && ".join("%s >= r_%s_lo%d && %s <= r_%s_hi%d" % (
                     qs[d], nm, d, qs[d], nm, d) for d in range(nd))
             cond = " && ".join(x for x in [own, flag or ""] if x)
             idx = gidx or " + ".join(
@@ -1846,8 +1872,11 @@ class ReductionGen(object):
             ctx.push()
             tgt = red.accumulate_ref.arguments
             tbind = dict(rbind)
+            # a condition on a function variable that is not a reduction
+            # variable restricts the target cell: bind it to the target index
             for fv, ta in zip(f.variables, tgt):
-                tbind[fv] = _subst(ta, rbind)
+                if all(fv is not rv for rv in rvars):
+                    tbind[fv] = _subst(ta, rbind)
             w.open("")
             for d, ta in enumerate(tgt):
                 w("const int c%d = %s;" % (d, ctx.expr(ta, rbind)))

@@ -499,6 +499,9 @@ def plan_stencil(pipeline, comps):
                             "anchor %s" % (n.name, anchor.name))
         off = anchor.ndims - n.ndims
         n.owned_map = [off + d for d in range(n.ndims)]
+    for n in nodes:
+        # materialized consumers read only where their Case holds
+        n.case_box = case_box(n.func) if n.role in ('out', 'smem') else None
     plan.nodes = nodes
     plan.node_of = node_of
 
@@ -564,6 +567,49 @@ def _domain_vals(func, env):
     return out
 
 
+def case_box(func):
+    """Per-dimension (lower-bound exprs, upper-bound exprs) of the single
+    box-shaped Case of ``func`` (None when it has several pieces, a plain
+    expression, or a condition that is not a box).  A consumer only reads
+    its producers where its Case holds, so footprints are computed over
+    the consumer's region intersected with this box."""
+    from .pipe import body_parts
+    from .bounds import part_boxes
+    parts = body_parts(func)
+    if len(parts) != 1 or parts[0][0] is None or parts[0][2] is not None:
+        return None
+    boxes = part_boxes(func)
+    if len(boxes) != 1 or not boxes[0][0].exact:
+        return None
+    b = boxes[0][0]
+    return [(b.lo[v], b.hi[v]) for v in func.variables]
+
+
+def case_restricted(node, region, env, constant_only=False):
+    """A node's region intersected with its Case box.  With
+    ``constant_only`` (static-extent simulation at far tile origins) only
+    bounds that do not depend on parameters are applied."""
+    lo, hi = region
+    cb = getattr(node, 'case_box', None)
+    if not cb:
+        return lo, hi
+    lo = list(lo)
+    hi = list(hi)
+    env2 = dict((k, v * 3 + 17) for k, v in env.items())
+    for d, (los, his) in enumerate(cb):
+        for e in los:
+            v = try_eval_int(e, env)
+            if v is None or (constant_only and try_eval_int(e, env2) != v):
+                continue
+            lo[d] = np.maximum(lo[d], v)
+        for e in his:
+            v = try_eval_int(e, env)
+            if v is None or (constant_only and try_eval_int(e, env2) != v):
+                continue
+            hi[d] = np.minimum(hi[d], v)
+    return lo, hi
+
+
 def infer_regions(plan, anchor_box, env, clamp=True, tile_first=None):
     """Region of every node for one tile (numpy-vectorizable: box bounds may
     be arrays).  ``anchor_box``: [(lo, hi)] per anchor dim.  ``tile_first``:
@@ -599,7 +645,8 @@ def infer_regions(plan, anchor_box, env, clamp=True, tile_first=None):
             lo = [np.maximum(l, dom[d][0]) for d, l in enumerate(lo)]
             hi = [np.minimum(h, dom[d][1]) for d, h in enumerate(hi)]
         for m, fns in n.uses:
-            mlo, mhi = regions[m.func]
+            mlo, mhi = case_restricted(m, regions[m.func], env,
+                                       constant_only=not clamp)
             nonempty = np.ones_like(np.asarray(mlo[0]), dtype=bool) \
                 if mlo else True
             for d in range(len(mlo)):
@@ -651,12 +698,25 @@ def _static_extents(plan, env):
             period = MAX_PERIOD
     plan.period = period
     exts = []
+    adom = _domain_vals(plan.anchor, env)
     for base in (period * (1 << 22), period * (1 << 23) + period * 7):
-        r = np.arange(period, dtype=np.int64)
+        # anchor dims of constant extent: their actual tiles; parametric
+        # dims: every residue of the origin, far from any border
+        axes = []
+        for k, t in enumerate(plan.tile):
+            if _const_extent(plan.anchor.domain[k], env) is not None:
+                lo0, hi0 = adom[k]
+                axes.append(np.arange(lo0, hi0 + 1, t, dtype=np.int64))
+            else:
+                axes.append(base + np.arange(period, dtype=np.int64))
+        grids = np.meshgrid(*axes, indexing='ij')
         box = []
         for k, t in enumerate(plan.tile):
-            lo = base + r
-            box.append((lo, lo + t - 1))
+            lo = grids[k].ravel()
+            hi = lo + t - 1
+            if _const_extent(plan.anchor.domain[k], env) is not None:
+                hi = np.minimum(hi, adom[k][1])
+            box.append((lo, hi))
         regs = infer_regions(plan, box, env, clamp=False)
         cur = {}
         for n in plan.nodes:
