@@ -7,18 +7,21 @@ from .harris import build_harris
 from .unsharp_mask import build_unsharp
 from .campipe import build_campipe
 from .bilateral_grid import build_bilateral
+from .pyramid_blend import build_pyramid
 
 HARRIS = dict(tile_sizes=(32, 64), options=('rblock=4',))
 UNSHARP = dict(tile_sizes=(32, 128), options=('rblock=8',))
 CAMPIPE = dict(tile_sizes=(32, 128), group_size=5, options=('rblock=4',))
 BILATERAL = dict(tile_sizes=(1, 32, 64), group_size=5,
                  options=(('red_tile', (32, 256)), 'rblock=4'))
+PYRAMID = dict(tile_sizes=(16, 128), group_size=10, options=('rblock=4',))
 
 _BUILDERS = {
     "harris": (build_harris, HARRIS),
     "unsharp": (build_unsharp, UNSHARP),
     "campipe": (build_campipe, CAMPIPE),
     "bilateral": (build_bilateral, BILATERAL),
+    "pyramid": (build_pyramid, PYRAMID),
 }
 
 _cache = {}

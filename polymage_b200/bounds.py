@@ -222,6 +222,66 @@ def expr_range(expr, ranges, env):
         return None
 
 
+def modular_restriction(cond):
+    """``(v, k, r)`` when ``cond`` is ``v % k == r`` (or ``!=`` with k = 2,
+    i.e. the other residue) for a loop variable ``v`` and constants k > 0,
+    0 <= r < k; else None.  The reference splits a Select on such a
+    condition into one domain per arm (sandbox/poly.py:761-879)."""
+    from .expr_ast import AbstractBinaryOpNode
+    if cond.conditional not in ('==', '!='):
+        return None
+    lhs = Value.numericToValue(cond.lhs)
+    rhs = Value.numericToValue(cond.rhs)
+    if not (isinstance(lhs, AbstractBinaryOpNode) and lhs.op == '%'):
+        return None
+    v = lhs.left
+    k = Value.numericToValue(lhs.right)
+    if not (isinstance(v, C.Variable) and not isinstance(v, C.Parameter)):
+        return None
+    if not (isinstance(k, Value) and isinstance(k.value, int) and
+            k.value > 0 and isinstance(rhs, Value) and
+            isinstance(rhs.value, int) and 0 <= rhs.value < k.value):
+        return None
+    if cond.conditional == '==':
+        return (v, k.value, rhs.value)
+    if k.value == 2:
+        return (v, 2, 1 - rhs.value)
+    return None
+
+
+def refs_with_residues(expr, restr=()):
+    """[(reference, ((v, k, r), ...))]: every reference of ``expr`` with the
+    residue classes its enclosing Select arms restrict variables to."""
+    out = []
+    if isinstance(expr, C.Reference):
+        out.append((expr, tuple(restr)))
+        for a in expr.arguments:
+            out += refs_with_residues(a, restr)
+        return out
+    if isinstance(expr, C.Select):
+        m = modular_restriction(expr.condition)
+        out += refs_with_residues(expr.condition, restr)
+        if m is not None:
+            v, k, r = m
+            other = (v, k, 1 - r) if k == 2 else None
+            out += refs_with_residues(expr.true_expression,
+                                      tuple(restr) + (m,))
+            out += refs_with_residues(expr.false_expression,
+                                      tuple(restr) + ((other,) if other
+                                                      else ()))
+            return out
+    for ch in (expr.children() if hasattr(expr, 'children') else []):
+        out += refs_with_residues(ch, restr)
+    return out
+
+
+def restrict_range(lo, hi, k, r):
+    """[lo, hi] shrunk to its extreme members congruent to r mod k."""
+    lo2 = lo + ((r - lo) % k)
+    hi2 = hi - ((hi - r) % k)
+    return lo2, hi2
+
+
 def bounds_check_pass(pipeline):
     """Check every reference of every compute object at the parameter
     estimates; record the symbolic checks for the run-time validator."""
@@ -236,22 +296,29 @@ def bounds_check_pass(pipeline):
                 continue
             if any(lo > hi for lo, hi in rng.values()):
                 continue
-            refs = list(expr.collect(C.Reference))
+            refs = refs_with_residues(expr)
             if cond is not None:
-                refs += cond.collect(C.Reference)
+                refs += [(r, ()) for r in cond.collect(C.Reference)]
             if red is not None:
-                refs += [red.accumulate_ref]
+                refs += [(red.accumulate_ref, ())]
                 for a in red.accumulate_ref.arguments:
-                    refs += a.collect(C.Reference)
-            for ref in refs:
+                    refs += [(r, ()) for r in a.collect(C.Reference)]
+            for ref, restr in refs:
                 g = ref.objectRef
                 is_target = (red is not None and ref is red.accumulate_ref)
+                rr = dict(rng)
+                for (v, k, r) in restr:
+                    if v in rr:
+                        rr[v] = restrict_range(rr[v][0], rr[v][1], k, r)
+                if any(lo > hi for lo, hi in rr.values()):
+                    continue
                 for dim, (arg, dom) in enumerate(zip(ref.arguments,
                                                      g.domain)):
-                    r = expr_range(arg, rng, env)
+                    r = expr_range(arg, rr, env)
                     if r is None:
                         continue
-                    checks.append((comp, box, arg, g, dim, is_target))
+                    checks.append((comp, box, arg, g, dim, is_target,
+                                   restr))
                     dlo = eval_int(dom.lowerBound, env)
                     dhi = eval_int(dom.upperBound, env)
                     if r[0] < dlo or r[1] > dhi:

@@ -415,8 +415,9 @@ class PipelineGen(object):
                   "return PM_ERR_PARAMS;" % (hi, lo))
         checks = getattr(self.p, '_bounds_checks', [])
         seen = set()
-        for (comp, box, arg, g, dim, is_target) in checks:
-            key = (id(comp), id(box), str(arg), id(g), dim)
+        for (comp, box, arg, g, dim, is_target, restr) in checks:
+            key = (id(comp), id(box), str(arg), id(g), dim,
+                   tuple((id(v), k, r) for v, k, r in restr))
             if key in seen:
                 continue
             seen.add(key)
@@ -433,6 +434,11 @@ class PipelineGen(object):
                 hi = his[0]
                 for x in his[1:]:
                     hi = "isl_min_i(%s, %s)" % (hi, x)
+                for (rv, k, r) in restr:
+                    if rv is v:
+                        # the Select arm only runs on v = r (mod k)
+                        lo = "pm_next_res(%s, %d, %d)" % (lo, k, r)
+                        hi = "pm_prev_res(%s, %d, %d)" % (hi, k, r)
                 w("const int %s_lo = %s, %s_hi = %s;" % (_vn(v), lo, _vn(v),
                                                           hi))
             empt = " || ".join("%s_lo > %s_hi" % (_vn(v), _vn(v))
@@ -2240,6 +2246,12 @@ def generate_code_for_pipeline(pipeline):
     w("static inline long long pm_llmax(long long a, long long b) { return a "
       "> b ? a : b; }")
     w("static inline int isl_min_i(int a, int b) { return a < b ? a : b; }")
+    w("static inline int pm_mod(int a, int k) { int m = a % k; return m < 0 "
+      "? m + k : m; }")
+    w("static inline int pm_next_res(int lo, int k, int r) { return lo + "
+      "pm_mod(r - lo, k); }")
+    w("static inline int pm_prev_res(int hi, int k, int r) { return hi - "
+      "pm_mod(hi - r, k); }")
     w("static inline int isl_max_i(int a, int b) { return a > b ? a : b; }")
     w("static bool pm_use_tma() { static int v = -1; if (v < 0) { const char*"
       " e = getenv(\"PM_DISABLE_TMA\"); v = (e && e[0] == '1') ? 0 : 1; } "
