@@ -1,0 +1,143 @@
+"""Tune the shipped pipelines on synthetic inputs of their benchmark sizes.
+
+  python -m polymage_b200.autotune --app unsharp --db timing_db.jsonl
+  python -m polymage_b200.autotune --app harris --learned model.npz --k 5
+
+Exhaustive mode runs ``tuner.generate`` + ``tuner.execute`` over the
+reference's search space (15 tile shapes x 5 group sizes, as the
+reference's app tuners use: harris/app_tuner.py:33-54) times the register
+blocking options, appending every measurement to the timing database.
+Learned mode ranks the same space with a trained cost model and times only
+its top-k.
+"""
+
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+
+from . import tuner
+from .apps.harris import harris_pipe
+from .apps.unsharp_mask import unsharp_mask
+from .apps.campipe import camera_pipe
+from .apps.bilateral_grid import bilateral_grid
+from .apps.pyramid_blend import pyramid_blending
+from .constructs import Condition
+
+
+def app_setup(app, seed=0):
+    """(tuner arg dict, pipe arg data) for one shipped pipeline."""
+    rng = np.random.default_rng(seed)
+    d = {}
+    if app == 'harris':
+        out = harris_pipe(d)
+        rows = cols = 2048
+        est = [(d['R'], rows - 2), (d['C'], cols - 2)]
+        data = {'R': rows - 2, 'C': cols - 2,
+                'img': rng.random((rows, cols), dtype=np.float32),
+                'harris': np.zeros((rows, cols), np.float32)}
+    elif app == 'unsharp':
+        out = unsharp_mask(d)
+        R = C = 4096
+        est = [(d['R'], R), (d['C'], C)]
+        data = {'R': R, 'C': C, 'threshold': 0.001, 'weight': 3.0,
+                'img': rng.random((3, R + 4, C + 4), dtype=np.float32),
+                'mask': np.zeros((3, R, C), np.float32)}
+    elif app == 'campipe':
+        out = camera_pipe(d)
+        R, C = 1968, 2592
+        est = [(d['R'], R), (d['C'], C)]
+        m3 = np.array([[1.6697, -0.2693, -0.4004, -42.4346],
+                       [-0.3576, 1.0615, 1.5949, -37.1158],
+                       [-0.2175, -1.8751, 6.9640, -26.6970]], np.float32)
+        m7 = np.array([[2.2997, -0.4478, 0.1706, -39.0923],
+                       [-0.3826, 1.5906, -0.2080, -25.4311],
+                       [-0.0888, -0.7344, 2.2832, -20.0826]], np.float32)
+        data = {'C': C, 'R': R, 'colour_temp': 3700.0, 'contrast': 50.0,
+                'gamma': 2.0,
+                'img': rng.integers(0, 1024, (R, C), dtype=np.int16),
+                'matrix_3200': m3, 'matrix_7000': m7,
+                'process': np.zeros((3, R - 48, C - 64), np.uint8)}
+    elif app == 'bilateral':
+        out = bilateral_grid(d)
+        rows, cols = 1536, 2560
+        est = [(d['R'], rows), (d['C'], cols)]
+        data = {'rows': rows, 'cols': cols,
+                'input': rng.random((rows, cols), dtype=np.float32),
+                'filtered': np.zeros((1, rows, cols), np.float32)}
+    elif app == 'pyramid':
+        out = pyramid_blending(d)
+        R = C = 2108
+        est = [(d['R'], R), (d['C'], C)]
+        data = {'R': R, 'C': C,
+                'img1': rng.random((3, R, C), dtype=np.float32),
+                'img2': rng.random((3, R, C), dtype=np.float32),
+                'mask': rng.random((R, C), dtype=np.float32),
+                'blend': np.zeros((3, R - 60, C - 60), np.float32)}
+    else:
+        raise ValueError(app)
+    arg = {'_tuner_app_name': app, '_tuner_live_outs': [out],
+           '_tuner_param_estimates': est,
+           '_tuner_param_constraints': [Condition(p, '==', v)
+                                        for p, v in est],
+           '_tuner_tile_size_configs': tuner.DEFAULT_TILES,
+           '_tuner_group_size_configs': tuner.DEFAULT_GROUPS,
+           '_tuner_option_configs': [['rblock=4']],
+           '_tuner_pipe_arg_data': data,
+           '_tuner_debug_flag': False}
+    if app == 'bilateral':
+        arg['_tuner_opts'] = [('red_tile', (32, 256))]
+    return arg
+
+
+def exhaustive(app, db, dst, nruns=5, option_configs=None):
+    a = app_setup(app)
+    if option_configs is not None:
+        a['_tuner_option_configs'] = option_configs
+    a['_tuner_dst_path'] = dst
+    a['_tuner_db'] = db
+    t0 = time.time()
+    src, n, pipe = tuner.generate(a)
+    t1 = time.time()
+    a['_tuner_src_path'] = src
+    a['_tuner_pipe'] = pipe
+    a['_tuner_nruns'] = nruns
+    rep = tuner.execute(a)
+    t2 = time.time()
+    rep['generate_s'] = t1 - t0
+    rep['wall_s'] = t2 - t0
+    return rep
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--app', required=True)
+    ap.add_argument('--db', default='timing_db.jsonl')
+    ap.add_argument('--dst', default='/tmp')
+    ap.add_argument('--nruns', type=int, default=5)
+    ap.add_argument('--learned', default=None)
+    ap.add_argument('--k', type=int, default=5)
+    ap.add_argument('--report', default=None)
+    args = ap.parse_args()
+    if args.learned:
+        from .costmodel import CostModel, learned_tune
+        model = CostModel.load(args.learned)
+        a = app_setup(args.app)
+        a['_tuner_dst_path'] = args.dst
+        a['_tuner_nruns'] = args.nruns
+        rep, wall = learned_tune(a, model, k=args.k)
+        rep['wall_s'] = wall
+    else:
+        rep = exhaustive(args.app, args.db, args.dst, args.nruns)
+    if args.report:
+        with open(args.report, 'w') as f:
+            json.dump(rep, f, indent=1)
+    best = rep['results'][0] if rep['results'] else None
+    print(json.dumps({'app': args.app, 'wall_s': rep.get('wall_s'),
+                      'best': best, 'n': len(rep['results'])}))
+
+
+if __name__ == '__main__':
+    main()

@@ -99,6 +99,26 @@ def compile_module(module, out_dir=None, verbose=False, force=False):
     return so
 
 
+def compile_source(name, path, out_dir=None, verbose=False):
+    """Compile a standalone CUDA source of this package (e.g. the cost
+    model's kernels) into ``libpm_<name>_<hash>.so``."""
+    out_dir = out_dir or GEN_DIR
+    os.makedirs(out_dir, exist_ok=True)
+    with open(path, "rb") as f:
+        src = f.read()
+    h = hashlib.sha1(src)
+    h.update(_runtime_hash().encode())
+    h.update(" ".join(ARCH_FLAGS + NVCC_FLAGS).encode())
+    so = os.path.join(out_dir, "libpm_%s_%s.so" % (name, h.hexdigest()[:16]))
+    if os.path.exists(so):
+        return so
+    tmp = so + ".tmp%d" % os.getpid()
+    _run([NVCC] + ARCH_FLAGS + NVCC_FLAGS + ["-I", CSRC, "-shared", path,
+                                             "-o", tmp], verbose)
+    os.replace(tmp, so)
+    return so
+
+
 def build_pipeline(pipeline, out_dir=None, verbose=False):
     from .runtime import CompiledPipeline
     module = pipeline.generate_code()

@@ -1,0 +1,230 @@
+"""Learned cost model for the tuner.
+
+A small MLP (FP32, three hidden layers of 128, ReLU) maps the plan
+features of a pipeline configuration (group structure, tile sizes, halo,
+shared-memory bytes, threads, recompute cost ... -- ``tuner.
+pipeline_features``) to its log kernel time relative to the other
+configurations of the same pipeline and input.  It is trained on the GPU by
+the hand-written kernels of ``csrc/mlp.cu`` (forward, backward, Adam) on the
+measurements the tuner appends to its timing database, and ranks
+configurations so that only the top-k are compiled and timed
+(``learned_tune``); the exhaustive tuner stays as the fallback and as the
+judge of the ranking.
+"""
+
+import ctypes
+import json
+import math
+import os
+import time
+
+import numpy as np
+
+from .build import compile_source, GEN_DIR, CSRC
+
+FEATURES = ['ngroups', 'nstencil', 'nred', 'stages', 'smem_max', 'smem_sum',
+            'halo_max', 'redund_sum', 'tile_inner', 'tile_outer', 'threads',
+            'cost_sum', 'nsmem', 'nstage_in', 'ninline', 'group_size',
+            'tile0', 'tile1', 'rblock', 'log_pixels']
+HIDDEN = 128
+
+_lib = None
+
+
+def lib():
+    """The cost model's CUDA library (built in-tree on first use)."""
+    global _lib
+    if _lib is None:
+        so = compile_source("mlp", os.path.join(CSRC, "mlp.cu"))
+        L = ctypes.CDLL(so)
+        L.pm_mlp_param_count.restype = ctypes.c_long
+        L.pm_mlp_param_count.argtypes = [ctypes.c_int, ctypes.c_int]
+        L.pm_mlp_act_count.restype = ctypes.c_long
+        L.pm_mlp_act_count.argtypes = [ctypes.c_int, ctypes.c_int]
+        L.pm_mlp_work_count.restype = ctypes.c_long
+        L.pm_mlp_work_count.argtypes = [ctypes.c_int, ctypes.c_int]
+        L.pm_mlp_forward.argtypes = [ctypes.c_void_p, ctypes.c_int,
+                                     ctypes.c_int, ctypes.c_void_p,
+                                     ctypes.c_int, ctypes.c_void_p,
+                                     ctypes.c_void_p, ctypes.c_void_p]
+        L.pm_mlp_backward.argtypes = [ctypes.c_void_p, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_void_p,
+                                      ctypes.c_void_p, ctypes.c_int] + \
+            [ctypes.c_void_p] * 5
+        L.pm_mlp_adam.argtypes = [ctypes.c_void_p] * 4 + \
+            [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+             ctypes.c_float, ctypes.c_void_p]
+        _lib = L
+    return _lib
+
+
+def featurize(features, cfg, pixels):
+    """Feature vector (log-scaled) of one configuration."""
+    f = dict(features)
+    tile = list(cfg['tile'])
+    f['group_size'] = cfg['group_size']
+    f['tile0'] = tile[-2] if len(tile) > 1 else 1
+    f['tile1'] = tile[-1]
+    rb = 4
+    for o in cfg.get('options', []):
+        if isinstance(o, str) and o.startswith('rblock='):
+            rb = int(o.split('=')[1])
+    f['rblock'] = rb
+    f['log_pixels'] = math.log(max(pixels, 1))
+    return np.array([math.log1p(max(float(f.get(k, 0.0)), 0.0))
+                     for k in FEATURES], np.float32)
+
+
+def pixels_of(data_key):
+    """Pixel count of a timing-database row's input (largest array)."""
+    try:
+        shapes = json.loads(data_key)
+    except ValueError:
+        return 1
+    best = 1
+    for _, s in shapes:
+        n = 1
+        for d in s[-2:]:
+            n *= d
+        best = max(best, n)
+    return best
+
+
+def relative_targets(rows):
+    """log(ms) minus the mean log(ms) of the row's (app, input) group."""
+    groups = {}
+    for r in rows:
+        groups.setdefault((r['app'], r['data']), []).append(math.log(r['ms']))
+    means = dict((k, sum(v) / len(v)) for k, v in groups.items())
+    return np.array([math.log(r['ms']) - means[(r['app'], r['data'])]
+                     for r in rows], np.float32)
+
+
+class CostModel(object):
+    def __init__(self, D=len(FEATURES), H=HIDDEN, seed=0):
+        import torch
+        self.D, self.H = D, H
+        L = lib()
+        n = L.pm_mlp_param_count(D, H)
+        rng = np.random.default_rng(seed)
+        p = np.zeros(n, np.float32)
+        # He initialization per layer
+        o = 0
+        for fan_in, fan_out in ((D, H), (H, H), (H, H), (H, 1)):
+            w = rng.normal(0, math.sqrt(2.0 / fan_in), fan_out * fan_in)
+            p[o:o + w.size] = w
+            o += w.size + fan_out
+        self.dev = torch.device('cuda', torch.cuda.current_device())
+        self.params = torch.from_numpy(p).to(self.dev)
+        self.mu = np.zeros(D, np.float32)
+        self.sd = np.ones(D, np.float32)
+        self.history = []
+
+    def _x(self, X):
+        import torch
+        Xn = (np.asarray(X, np.float32) - self.mu) / self.sd
+        return torch.from_numpy(np.ascontiguousarray(Xn)).to(self.dev)
+
+    def fit(self, X, y, epochs=600, lr=2e-3, weight_decay=1e-4):
+        """Full-batch Adam on the GPU; returns the loss curve."""
+        import torch
+        X = np.asarray(X, np.float32)
+        self.mu = X.mean(0)
+        self.sd = X.std(0) + 1e-3
+        L = lib()
+        B = X.shape[0]
+        xd = self._x(X)
+        yd = torch.from_numpy(np.asarray(y, np.float32)).to(self.dev)
+        acts = torch.zeros(L.pm_mlp_act_count(B, self.H), device=self.dev)
+        work = torch.zeros(L.pm_mlp_work_count(B, self.H), device=self.dev)
+        grads = torch.zeros_like(self.params)
+        m = torch.zeros_like(self.params)
+        v = torch.zeros_like(self.params)
+        loss = torch.zeros(1, device=self.dev)
+        s = torch.cuda.current_stream().cuda_stream
+        losses = []
+        for t in range(1, epochs + 1):
+            st = L.pm_mlp_backward(self.params.data_ptr(), self.D, self.H,
+                                   xd.data_ptr(), yd.data_ptr(), B,
+                                   acts.data_ptr(), work.data_ptr(),
+                                   grads.data_ptr(), loss.data_ptr(), s)
+            st |= L.pm_mlp_adam(self.params.data_ptr(), grads.data_ptr(),
+                                m.data_ptr(), v.data_ptr(), self.D, self.H,
+                                t, lr, weight_decay, s)
+            if st:
+                raise RuntimeError("cost model kernels failed")
+            if t % 50 == 0 or t == 1:
+                losses.append(float(loss.item()))
+        self.history = losses
+        return losses
+
+    def predict(self, X):
+        import torch
+        L = lib()
+        X = np.asarray(X, np.float32)
+        B = X.shape[0]
+        xd = self._x(X)
+        acts = torch.zeros(L.pm_mlp_act_count(B, self.H), device=self.dev)
+        out = torch.zeros(B, device=self.dev)
+        st = L.pm_mlp_forward(self.params.data_ptr(), self.D, self.H,
+                              xd.data_ptr(), B, acts.data_ptr(),
+                              out.data_ptr(),
+                              torch.cuda.current_stream().cuda_stream)
+        if st:
+            raise RuntimeError("cost model forward failed")
+        return out.cpu().numpy()
+
+    def save(self, path):
+        np.savez(path, params=self.params.cpu().numpy(), mu=self.mu,
+                 sd=self.sd, D=self.D, H=self.H)
+
+    @classmethod
+    def load(cls, path):
+        import torch
+        z = np.load(path)
+        m = cls(int(z['D']), int(z['H']))
+        m.params = torch.from_numpy(z['params']).to(m.dev)
+        m.mu, m.sd = z['mu'], z['sd']
+        return m
+
+
+def train_from_rows(rows, exclude_app=None, epochs=600, seed=0):
+    rows = [r for r in rows if r['app'] != exclude_app]
+    X = np.stack([featurize(r['features'], r, pixels_of(r['data']))
+                  for r in rows])
+    y = relative_targets(rows)
+    model = CostModel(seed=seed)
+    model.fit(X, y, epochs=epochs)
+    return model
+
+
+def learned_tune(arg_data, model, k=5):
+    """Plan every configuration (no compilation), rank them with the model,
+    compile and time only the top-k; returns (report, wall seconds)."""
+    from . import tuner
+    t0 = time.time()
+    a = dict(arg_data)
+    app = a['_tuner_app_name']
+    name = a.get('_tuner_pipe_name') or app
+    configs = a.get('_tuner_configs') or tuner.enumerate_configs(
+        a.get('_tuner_tile_size_configs') or tuner.DEFAULT_TILES,
+        a.get('_tuner_group_size_configs') or tuner.DEFAULT_GROUPS,
+        a.get('_tuner_option_configs'))
+    data = a['_tuner_pipe_arg_data']
+    pix = pixels_of(tuner.data_key(data))
+    cand, feats = [], []
+    for cfg in configs:
+        try:
+            p = tuner.plan_config(a, cfg, name)
+        except Exception:
+            continue
+        cand.append(cfg)
+        feats.append(featurize(tuner.pipeline_features(p), cfg, pix))
+    pred = model.predict(np.stack(feats))
+    order = np.argsort(pred)[:k]
+    a['_tuner_configs'] = [cand[i] for i in order]
+    src, n, pipe = tuner.generate(a)
+    a['_tuner_src_path'] = src
+    a['_tuner_pipe'] = pipe
+    report = tuner.execute(a)
+    return report, time.time() - t0
