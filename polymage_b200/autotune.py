@@ -117,26 +117,47 @@ def main():
     ap.add_argument('--db', default='timing_db.jsonl')
     ap.add_argument('--dst', default='/tmp')
     ap.add_argument('--nruns', type=int, default=5)
-    ap.add_argument('--learned', default=None)
-    ap.add_argument('--k', type=int, default=5)
+    ap.add_argument('--learned', action='store_true',
+                    help='online learned tuning (cost model)')
+    ap.add_argument('--compare', action='store_true',
+                    help='learned tuning, then exhaustive tuning as judge')
+    ap.add_argument('--rounds', type=int, default=3)
+    ap.add_argument('--batch', type=int, default=2)
+    ap.add_argument('--options', default=None,
+                    help='JSON list of option lists to search over')
     ap.add_argument('--report', default=None)
     args = ap.parse_args()
-    if args.learned:
-        from .costmodel import CostModel, learned_tune
-        model = CostModel.load(args.learned)
+    opts = json.loads(args.options) if args.options else None
+    out = {'app': args.app}
+    if args.learned or args.compare:
+        from .costmodel import learned_tune
         a = app_setup(args.app)
-        a['_tuner_dst_path'] = args.dst
+        if opts is not None:
+            a['_tuner_option_configs'] = opts
+        a['_tuner_dst_path'] = os.path.join(args.dst, 'learned')
         a['_tuner_nruns'] = args.nruns
-        rep, wall = learned_tune(a, model, k=args.k)
-        rep['wall_s'] = wall
-    else:
-        rep = exhaustive(args.app, args.db, args.dst, args.nruns)
+        lr = learned_tune(a, rounds=args.rounds, batch=args.batch,
+                          shipped_app=args.app)
+        out['learned'] = {'best': lr['best'], 'best_ms': lr['best_ms'],
+                          'wall_s': lr['wall_s'], 'plan_s': lr['plan_s'],
+                          'measured': len(lr['measured']),
+                          'candidates': lr['candidates']}
+    if not args.learned or args.compare:
+        rep = exhaustive(args.app, args.db, args.dst, args.nruns,
+                         option_configs=opts)
+        best = rep['results'][0] if rep['results'] else None
+        out['exhaustive'] = {'best': best, 'wall_s': rep['wall_s'],
+                             'n': len(rep['results'])}
+    if args.compare and out['exhaustive']['best'] and \
+            out['learned']['best_ms']:
+        out['time_ratio'] = out['learned']['best_ms'] / \
+            out['exhaustive']['best']['ms']
+        out['wall_ratio'] = out['learned']['wall_s'] / \
+            out['exhaustive']['wall_s']
     if args.report:
         with open(args.report, 'w') as f:
-            json.dump(rep, f, indent=1)
-    best = rep['results'][0] if rep['results'] else None
-    print(json.dumps({'app': args.app, 'wall_s': rep.get('wall_s'),
-                      'best': best, 'n': len(rep['results'])}))
+            json.dump(out, f, indent=1)
+    print(json.dumps(out))
 
 
 if __name__ == '__main__':

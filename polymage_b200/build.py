@@ -14,10 +14,11 @@ flags.
 import hashlib
 import os
 import subprocess
+import threading
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
-GEN_DIR = os.path.join(HERE, "_gen")
+GEN_DIR = os.environ.get("PM_GEN_DIR") or os.path.join(HERE, "_gen")
 
 NVCC = os.environ.get("PM_NVCC", "nvcc")
 CXX = os.environ.get("PM_CXX", "g++")
@@ -66,37 +67,50 @@ def library_path(module, out_dir=None):
     return os.path.join(out_dir, "libpm_%s_%s.so" % (module.name, tag)), tag
 
 
+_locks = {}
+_locks_guard = threading.Lock()
+
+
+def _lock_for(path):
+    with _locks_guard:
+        return _locks.setdefault(path, threading.Lock())
+
+
 def compile_module(module, out_dir=None, verbose=False, force=False):
-    """Compile a CudaModule; returns the path of the shared library."""
+    """Compile a CudaModule; returns the path of the shared library.  Safe
+    to call concurrently (identical modules compile once; temporaries have
+    per-process, per-thread names)."""
     out_dir = out_dir or GEN_DIR
     os.makedirs(out_dir, exist_ok=True)
     so, tag = library_path(module, out_dir)
-    if os.path.exists(so) and not force:
+    with _lock_for(so):
+        if os.path.exists(so) and not force:
+            return so
+        base = os.path.join(out_dir, "pm_%s_%s" % (module.name, tag))
+        uniq = "%s.%d.%d" % (base, os.getpid(), threading.get_ident())
+        with open(base + ".cu", "w") as f:
+            f.write(module.source)
+        with open(base + ".h", "w") as f:
+            f.write(module.header)
+        objs = []
+        _run([NVCC] + ARCH_FLAGS + NVCC_FLAGS +
+             ["-I", CSRC, "-c", base + ".cu", "-o", uniq + ".o"], verbose)
+        objs.append(uniq + ".o")
+        if module.host_source:
+            with open(base + "_host.cpp", "w") as f:
+                f.write(module.host_source)
+            _run([CXX] + CXX_FLAGS + ["-c", base + "_host.cpp", "-o",
+                                      uniq + "_host.o"], verbose)
+            objs.append(uniq + "_host.o")
+        tmp = uniq + ".so.tmp"
+        _run([NVCC] + ARCH_FLAGS + ["-shared", "-o", tmp] + objs, verbose)
+        os.replace(tmp, so)
+        for o in objs:
+            try:
+                os.remove(o)
+            except OSError:
+                pass
         return so
-    base = os.path.join(out_dir, "pm_%s_%s" % (module.name, tag))
-    with open(base + ".cu", "w") as f:
-        f.write(module.source)
-    with open(base + ".h", "w") as f:
-        f.write(module.header)
-    objs = []
-    _run([NVCC] + ARCH_FLAGS + NVCC_FLAGS + ["-I", CSRC, "-c", base + ".cu",
-                                             "-o", base + ".o"], verbose)
-    objs.append(base + ".o")
-    if module.host_source:
-        with open(base + "_host.cpp", "w") as f:
-            f.write(module.host_source)
-        _run([CXX] + CXX_FLAGS + ["-c", base + "_host.cpp", "-o",
-                                  base + "_host.o"], verbose)
-        objs.append(base + "_host.o")
-    tmp = so + ".tmp%d" % os.getpid()
-    _run([NVCC] + ARCH_FLAGS + ["-shared", "-o", tmp] + objs, verbose)
-    os.replace(tmp, so)
-    for o in objs:
-        try:
-            os.remove(o)
-        except OSError:
-            pass
-    return so
 
 
 def compile_source(name, path, out_dir=None, verbose=False):

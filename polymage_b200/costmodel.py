@@ -198,33 +198,195 @@ def train_from_rows(rows, exclude_app=None, epochs=600, seed=0):
     return model
 
 
-def learned_tune(arg_data, model, k=5):
-    """Plan every configuration (no compilation), rank them with the model,
-    compile and time only the top-k; returns (report, wall seconds)."""
+DB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data",
+                       "timing_db_b200.jsonl")
+
+
+def signature(features, cfg):
+    """Configurations with equal signatures generate the same code."""
+    return json.dumps([sorted(features.items()), list(cfg['tile']),
+                       [list(o) if isinstance(o, tuple) else o
+                        for o in cfg.get('options', [])]])
+
+
+def app_normalized(X, groups):
+    """Features minus their mean over the configurations of the same
+    pipeline and input (the targets are relative to that group too)."""
+    X = np.array(X, np.float32)
+    out = X.copy()
+    for g in set(groups):
+        idx = [i for i, h in enumerate(groups) if h == g]
+        out[idx] = X[idx] - X[idx].mean(0)
+    return out
+
+
+def db_training_set(rows, exclude_app=None):
+    """(X, y) of the timing database, one row per distinct plan, features
+    and targets relative to each (pipeline, input) group."""
+    uniq = {}
+    for r in rows:
+        if r['app'] == exclude_app:
+            continue
+        k = (r['app'], r['data'], signature(r['features'], r))
+        if k not in uniq or r['ms'] < uniq[k]['ms']:
+            uniq[k] = r
+    rs = list(uniq.values())
+    if not rs:
+        return np.zeros((0, len(FEATURES)), np.float32), np.zeros(0,
+                                                                   np.float32)
+    X = np.stack([featurize(r['features'], r, pixels_of(r['data']))
+                  for r in rs])
+    X = app_normalized(X, [(r['app'], r['data']) for r in rs])
+    return X, relative_targets(rs)
+
+
+def _plan_worker(job):
+    app, cfg = job
+    from .autotune import app_setup
+    from . import tuner
+    try:
+        p = tuner.plan_config(app_setup(app), cfg, app)
+        return tuner.pipeline_features(p)
+    except Exception:
+        return None
+
+
+def plan_candidates(arg_data, configs, jobs=None, app_for_workers=None):
+    """Plan features of every configuration (None for plans that fail).
+    Shipped pipelines are planned in parallel worker processes (spawned:
+    the workers rebuild the spec by name); others sequentially."""
+    from . import tuner
+    if app_for_workers is not None and len(configs) > 8:
+        import multiprocessing as mp
+        jobs = jobs or max(1, (os.cpu_count() or 2) - 1)
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(jobs) as pool:
+            return pool.map(_plan_worker,
+                            [(app_for_workers, c) for c in configs],
+                            chunksize=max(1, len(configs) // (4 * jobs)))
+    out = []
+    name = arg_data.get('_tuner_pipe_name') or arg_data['_tuner_app_name']
+    for cfg in configs:
+        try:
+            out.append(tuner.pipeline_features(
+                tuner.plan_config(arg_data, cfg, name)))
+        except Exception:
+            out.append(None)
+    return out
+
+
+def learned_tune(arg_data, db_rows=None, rounds=3, batch=2, epochs=200,
+                 repeat=20, seed=0, shipped_app=None, measure=None):
+    """Online learned tuning.  The model starts from the timing database
+    (other pipelines) and, each round, ranks the not yet measured distinct
+    plans, times the ``batch`` best predicted ones, and retrains with those
+    measurements (weighted ``repeat`` times).  ``measure(configs)`` returns
+    their times in ms (default: compile with ``tuner.generate`` and time
+    with ``tuner.execute``).  Returns a dict with the best configuration,
+    every measurement and the wall-clock seconds spent."""
     from . import tuner
     t0 = time.time()
     a = dict(arg_data)
     app = a['_tuner_app_name']
-    name = a.get('_tuner_pipe_name') or app
     configs = a.get('_tuner_configs') or tuner.enumerate_configs(
         a.get('_tuner_tile_size_configs') or tuner.DEFAULT_TILES,
         a.get('_tuner_group_size_configs') or tuner.DEFAULT_GROUPS,
         a.get('_tuner_option_configs'))
+    feats = plan_candidates(a, configs, app_for_workers=shipped_app)
     data = a['_tuner_pipe_arg_data']
     pix = pixels_of(tuner.data_key(data))
-    cand, feats = [], []
-    for cfg in configs:
-        try:
-            p = tuner.plan_config(a, cfg, name)
-        except Exception:
+    cand, seen = [], set()
+    for cfg, f in zip(configs, feats):
+        if f is None:
             continue
-        cand.append(cfg)
-        feats.append(featurize(tuner.pipeline_features(p), cfg, pix))
-    pred = model.predict(np.stack(feats))
-    order = np.argsort(pred)[:k]
-    a['_tuner_configs'] = [cand[i] for i in order]
-    src, n, pipe = tuner.generate(a)
-    a['_tuner_src_path'] = src
-    a['_tuner_pipe'] = pipe
-    report = tuner.execute(a)
-    return report, time.time() - t0
+        s = signature(f, cfg)
+        if s in seen:
+            continue
+        seen.add(s)
+        cand.append((cfg, f))
+    Xc = app_normalized(np.stack([featurize(f, c, pix) for c, f in cand]),
+                        [0] * len(cand))
+    if db_rows is None:
+        db_rows = tuner.load_db(DB_PATH)
+    Xb, yb = db_training_set(db_rows, exclude_app=app)
+    t_plan = time.time() - t0
+
+    if measure is None:
+        def measure(cfgs):
+            b = dict(a)
+            b['_tuner_configs'] = cfgs
+            src, n, pipe = tuner.generate(b)
+            b['_tuner_src_path'] = src
+            b['_tuner_pipe'] = pipe
+            rep = tuner.execute(b)
+            times = {}
+            for r in rep['results']:
+                times[json.dumps([r['tile'], r['group_size'], r['options']])
+                      ] = r['ms']
+            return [times.get(json.dumps([c['tile'], c['group_size'],
+                                          c['options']])) for c in cfgs]
+
+    measured = {}
+    for rd in range(rounds):
+        X, y = Xb, yb
+        idx = [i for i in measured if measured[i] is not None]
+        if len(idx) >= 2:
+            ym = np.log([measured[i] for i in idx])
+            ym = (ym - ym.mean()).astype(np.float32)
+            X = np.concatenate([Xb] + [Xc[idx]] * repeat)
+            y = np.concatenate([yb] + [ym] * repeat)
+        if len(X) == 0:
+            order = list(range(len(cand)))
+        else:
+            model = CostModel(seed=seed + rd)
+            model.fit(X, y, epochs=epochs)
+            order = list(np.argsort(model.predict(Xc)))
+        pick = [i for i in order if i not in measured][:batch]
+        if not pick:
+            break
+        times = measure([cand[i][0] for i in pick])
+        for i, ms in zip(pick, times):
+            measured[i] = ms
+    ok = [(ms, i) for i, ms in measured.items() if ms is not None]
+    best = min(ok) if ok else (None, None)
+    return {'app': app, 'best': cand[best[1]][0] if ok else None,
+            'best_ms': best[0], 'measured': [
+                {'config': cand[i][0], 'ms': ms} for i, ms in
+                measured.items()],
+            'candidates': len(cand), 'plan_s': t_plan,
+            'wall_s': time.time() - t0}
+
+
+def evaluate_on_db(rows, app, rounds=3, batch=2, seed=0):
+    """Replay ``learned_tune`` on recorded measurements of ``app`` (the
+    model never sees them except through its own picks); returns
+    (best picked ms / best recorded ms, number measured, distinct plans)."""
+    uniq = {}
+    for r in rows:
+        if r['app'] != app:
+            continue
+        k = signature(r['features'], r)
+        if k not in uniq or r['ms'] < uniq[k]['ms']:
+            uniq[k] = r
+    te = list(uniq.values())
+    Xc = app_normalized(np.stack([featurize(r['features'], r,
+                                            pixels_of(r['data']))
+                                  for r in te]), [0] * len(te))
+    Xb, yb = db_training_set(rows, exclude_app=app)
+    measured = {}
+    for rd in range(rounds):
+        X, y = Xb, yb
+        idx = list(measured)
+        if len(idx) >= 2:
+            ym = np.log([te[i]['ms'] for i in idx])
+            ym = (ym - ym.mean()).astype(np.float32)
+            X = np.concatenate([Xb] + [Xc[idx]] * 20)
+            y = np.concatenate([yb] + [ym] * 20)
+        model = CostModel(seed=seed + rd)
+        model.fit(X, y, epochs=200)
+        order = [i for i in np.argsort(model.predict(Xc)) if i not in
+                 measured]
+        for i in order[:batch]:
+            measured[i] = te[i]['ms']
+    best = min(r['ms'] for r in te)
+    return min(measured.values()) / best, len(measured), len(te)

@@ -112,7 +112,7 @@ def generate(_tuner_arg_data):
         try:
             entry['so'] = compile_module(mod)
             entry['status'] = 'built'
-        except BuildError as e:
+        except Exception as e:          # a failing build is skipped
             entry['status'] = 'build_failed'
             entry['error'] = str(e)[-300:]
         return entry
