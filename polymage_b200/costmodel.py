@@ -275,15 +275,87 @@ def plan_candidates(arg_data, configs, jobs=None, app_for_workers=None):
     return out
 
 
-def learned_tune(arg_data, db_rows=None, rounds=3, batch=2, epochs=200,
-                 repeat=20, seed=0, shipped_app=None, measure=None):
-    """Online learned tuning.  The model starts from the timing database
-    (other pipelines) and, each round, ranks the not yet measured distinct
-    plans, times the ``batch`` best predicted ones, and retrains with those
-    measurements (weighted ``repeat`` times).  ``measure(configs)`` returns
-    their times in ms (default: compile with ``tuner.generate`` and time
-    with ``tuner.execute``).  Returns a dict with the best configuration,
-    every measurement and the wall-clock seconds spent."""
+def _rblock(cfg):
+    for o in cfg.get('options', []):
+        if isinstance(o, str) and o.startswith('rblock='):
+            return int(o.split('=')[1])
+    return 4
+
+
+def neighbours(a, b):
+    """True when configuration ``a`` differs from ``b`` by one step of one
+    knob: a tile side halved or doubled, the register blocking, or the
+    group size."""
+    ta, tb = a['tile'], b['tile']
+    steps = 0
+    for x, y in ((ta[-2] if len(ta) > 1 else 1, tb[-2] if len(tb) > 1
+                  else 1), (ta[-1], tb[-1])):
+        if x != y:
+            steps += 1 if x in (2 * y, y // 2) else 9
+    if _rblock(a) != _rblock(b):
+        steps += 1
+    if a['group_size'] != b['group_size']:
+        steps += 1
+    return steps == 1
+
+
+class OnlineRanker(object):
+    """The online protocol shared by the live tuner and its replay on
+    recorded timings: an ensemble of cost models pretrained on other
+    pipelines' measurements, retrained on the GPU after every batch with
+    this pipeline's own measurements (weighted ``repeat`` times)."""
+
+    def __init__(self, Xc, Xb, yb, ensemble=3, epochs=200, repeat=20,
+                 seed=0):
+        self.Xc, self.Xb, self.yb = Xc, Xb, yb
+        self.ensemble, self.epochs, self.repeat = ensemble, epochs, repeat
+        self.seed = seed
+        self.measured = {}
+
+    def order(self):
+        idx = [i for i, ms in self.measured.items() if ms is not None]
+        X, y = self.Xb, self.yb
+        if len(idx) >= 2:
+            ym = np.log([self.measured[i] for i in idx])
+            ym = (ym - ym.mean()).astype(np.float32)
+            X = np.concatenate([self.Xb] + [self.Xc[idx]] * self.repeat)
+            y = np.concatenate([self.yb] + [ym] * self.repeat)
+        if len(X) == 0:
+            return list(range(len(self.Xc)))
+        pred = np.zeros(len(self.Xc), np.float32)
+        for e in range(self.ensemble):
+            m = CostModel(seed=self.seed * 100 + len(self.measured) * 7 + e)
+            m.fit(X, y, epochs=self.epochs)
+            pred += m.predict(self.Xc)
+        return [int(i) for i in np.argsort(pred)]
+
+    def run(self, cands, measure, batches=(4, 2), local=2):
+        for b in batches:
+            pick = [i for i in self.order() if i not in self.measured][:b]
+            if not pick:
+                break
+            for i, ms in zip(pick, measure(pick)):
+                self.measured[i] = ms
+        ok = [i for i, ms in self.measured.items() if ms is not None]
+        if ok and local:
+            bi = min(ok, key=lambda i: self.measured[i])
+            pick = [i for i in self.order() if i not in self.measured and
+                    neighbours(cands[i], cands[bi])][:local]
+            for i, ms in zip(pick, measure(pick) if pick else []):
+                self.measured[i] = ms
+        ok = [i for i, ms in self.measured.items() if ms is not None]
+        return min(ok, key=lambda i: self.measured[i]) if ok else None
+
+
+def learned_tune(arg_data, db_rows=None, batches=(4, 2), local=2,
+                 ensemble=3, seed=0, shipped_app=None, measure=None):
+    """Online learned tuning of one pipeline: plan every configuration of
+    the search space (no compilation), keep one per distinct plan, then
+    time only what the cost model ranks first (``OnlineRanker.run``).
+    ``measure(configs)`` returns their times in ms (default: compile with
+    ``tuner.generate`` and time with ``tuner.execute``).  Returns a dict
+    with the best configuration, every measurement and the wall-clock
+    seconds spent, planning included."""
     from . import tuner
     t0 = time.time()
     a = dict(arg_data)
@@ -293,9 +365,8 @@ def learned_tune(arg_data, db_rows=None, rounds=3, batch=2, epochs=200,
         a.get('_tuner_group_size_configs') or tuner.DEFAULT_GROUPS,
         a.get('_tuner_option_configs'))
     feats = plan_candidates(a, configs, app_for_workers=shipped_app)
-    data = a['_tuner_pipe_arg_data']
-    pix = pixels_of(tuner.data_key(data))
-    cand, seen = [], set()
+    pix = pixels_of(tuner.data_key(a['_tuner_pipe_arg_data']))
+    cands, cfeat, seen = [], [], set()
     for cfg, f in zip(configs, feats):
         if f is None:
             continue
@@ -303,63 +374,42 @@ def learned_tune(arg_data, db_rows=None, rounds=3, batch=2, epochs=200,
         if s in seen:
             continue
         seen.add(s)
-        cand.append((cfg, f))
-    Xc = app_normalized(np.stack([featurize(f, c, pix) for c, f in cand]),
-                        [0] * len(cand))
+        cands.append(cfg)
+        cfeat.append(featurize(f, cfg, pix))
+    Xc = app_normalized(np.stack(cfeat), [0] * len(cands))
     if db_rows is None:
         db_rows = tuner.load_db(DB_PATH)
     Xb, yb = db_training_set(db_rows, exclude_app=app)
     t_plan = time.time() - t0
 
-    if measure is None:
-        def measure(cfgs):
-            b = dict(a)
-            b['_tuner_configs'] = cfgs
-            src, n, pipe = tuner.generate(b)
-            b['_tuner_src_path'] = src
-            b['_tuner_pipe'] = pipe
-            rep = tuner.execute(b)
-            times = {}
-            for r in rep['results']:
-                times[json.dumps([r['tile'], r['group_size'], r['options']])
-                      ] = r['ms']
-            return [times.get(json.dumps([c['tile'], c['group_size'],
-                                          c['options']])) for c in cfgs]
+    def default_measure(idx):
+        b = dict(a)
+        b['_tuner_configs'] = [cands[i] for i in idx]
+        src, n, pipe = tuner.generate(b)
+        b['_tuner_src_path'] = src
+        b['_tuner_pipe'] = pipe
+        rep = tuner.execute(b)
+        got = dict((json.dumps([r['tile'], r['group_size'], r['options']]),
+                    r['ms']) for r in rep['results'])
+        return [got.get(json.dumps([cands[i]['tile'], cands[i]['group_size'],
+                                    cands[i]['options']])) for i in idx]
 
-    measured = {}
-    for rd in range(rounds):
-        X, y = Xb, yb
-        idx = [i for i in measured if measured[i] is not None]
-        if len(idx) >= 2:
-            ym = np.log([measured[i] for i in idx])
-            ym = (ym - ym.mean()).astype(np.float32)
-            X = np.concatenate([Xb] + [Xc[idx]] * repeat)
-            y = np.concatenate([yb] + [ym] * repeat)
-        if len(X) == 0:
-            order = list(range(len(cand)))
-        else:
-            model = CostModel(seed=seed + rd)
-            model.fit(X, y, epochs=epochs)
-            order = list(np.argsort(model.predict(Xc)))
-        pick = [i for i in order if i not in measured][:batch]
-        if not pick:
-            break
-        times = measure([cand[i][0] for i in pick])
-        for i, ms in zip(pick, times):
-            measured[i] = ms
-    ok = [(ms, i) for i, ms in measured.items() if ms is not None]
-    best = min(ok) if ok else (None, None)
-    return {'app': app, 'best': cand[best[1]][0] if ok else None,
-            'best_ms': best[0], 'measured': [
-                {'config': cand[i][0], 'ms': ms} for i, ms in
-                measured.items()],
-            'candidates': len(cand), 'plan_s': t_plan,
+    meas = (lambda idx: measure([cands[i] for i in idx])) if measure \
+        else default_measure
+    ranker = OnlineRanker(Xc, Xb, yb, ensemble=ensemble, seed=seed)
+    best = ranker.run(cands, meas, batches=batches, local=local)
+    return {'app': app,
+            'best': cands[best] if best is not None else None,
+            'best_ms': ranker.measured[best] if best is not None else None,
+            'measured': [{'config': cands[i], 'ms': ms}
+                         for i, ms in ranker.measured.items()],
+            'candidates': len(cands), 'plan_s': t_plan,
             'wall_s': time.time() - t0}
 
 
-def evaluate_on_db(rows, app, rounds=3, batch=2, seed=0):
-    """Replay ``learned_tune`` on recorded measurements of ``app`` (the
-    model never sees them except through its own picks); returns
+def evaluate_on_db(rows, app, batches=(4, 2), local=2, ensemble=3, seed=0):
+    """Replay ``learned_tune`` on recorded measurements of ``app``: the
+    ranker only learns the times of the configurations it picks.  Returns
     (best picked ms / best recorded ms, number measured, distinct plans)."""
     uniq = {}
     for r in rows:
@@ -373,20 +423,8 @@ def evaluate_on_db(rows, app, rounds=3, batch=2, seed=0):
                                             pixels_of(r['data']))
                                   for r in te]), [0] * len(te))
     Xb, yb = db_training_set(rows, exclude_app=app)
-    measured = {}
-    for rd in range(rounds):
-        X, y = Xb, yb
-        idx = list(measured)
-        if len(idx) >= 2:
-            ym = np.log([te[i]['ms'] for i in idx])
-            ym = (ym - ym.mean()).astype(np.float32)
-            X = np.concatenate([Xb] + [Xc[idx]] * 20)
-            y = np.concatenate([yb] + [ym] * 20)
-        model = CostModel(seed=seed + rd)
-        model.fit(X, y, epochs=200)
-        order = [i for i in np.argsort(model.predict(Xc)) if i not in
-                 measured]
-        for i in order[:batch]:
-            measured[i] = te[i]['ms']
-    best = min(r['ms'] for r in te)
-    return min(measured.values()) / best, len(measured), len(te)
+    ranker = OnlineRanker(Xc, Xb, yb, ensemble=ensemble, seed=seed)
+    best = ranker.run(te, lambda idx: [te[i]['ms'] for i in idx],
+                      batches=batches, local=local)
+    top = min(r['ms'] for r in te)
+    return ranker.measured[best] / top, len(ranker.measured), len(te)
