@@ -136,8 +136,8 @@ def main():
             a['_tuner_option_configs'] = opts
         a['_tuner_dst_path'] = os.path.join(args.dst, 'learned')
         a['_tuner_nruns'] = args.nruns
-        lr = learned_tune(a, rounds=args.rounds, batch=args.batch,
-                          shipped_app=args.app)
+        lr = learned_tune(a, batches=(args.batch * 2, args.batch),
+                          local=args.batch, shipped_app=args.app)
         out['learned'] = {'best': lr['best'], 'best_ms': lr['best_ms'],
                           'wall_s': lr['wall_s'], 'plan_s': lr['plan_s'],
                           'measured': len(lr['measured']),

@@ -255,15 +255,24 @@ def plan_candidates(arg_data, configs, jobs=None, app_for_workers=None):
     """Plan features of every configuration (None for plans that fail).
     Shipped pipelines are planned in parallel worker processes (spawned:
     the workers rebuild the spec by name); others sequentially."""
+    import sys
     from . import tuner
-    if app_for_workers is not None and len(configs) > 8:
+    main_file = getattr(sys.modules.get('__main__'), '__file__', None)
+    spawnable = main_file is not None and os.path.exists(main_file)
+    if app_for_workers is not None and len(configs) > 8 and spawnable:
         import multiprocessing as mp
         jobs = jobs or max(1, (os.cpu_count() or 2) - 1)
         ctx = mp.get_context("spawn")
-        with ctx.Pool(jobs) as pool:
-            return pool.map(_plan_worker,
-                            [(app_for_workers, c) for c in configs],
-                            chunksize=max(1, len(configs) // (4 * jobs)))
+        pool = ctx.Pool(jobs)
+        try:
+            res = pool.map_async(_plan_worker,
+                                 [(app_for_workers, c) for c in configs],
+                                 chunksize=max(1, len(configs) //
+                                               (4 * jobs)))
+            return res.get(timeout=600)
+        finally:
+            pool.terminate()
+            pool.join()
     out = []
     name = arg_data.get('_tuner_pipe_name') or arg_data['_tuner_app_name']
     for cfg in configs:
