@@ -14,6 +14,10 @@ int pipeline_pyramid_graph(int C, int R, void* img1, void* img2, void* mask, voi
 /* n images; iparams: n x 2 int params, fparams: n x 0 float params, each row in
  * name order; inputs: n x 3 device pointers, outputs: n x 1 device pointers */
 int pipeline_pyramid_batch(int n, const int* iparams, const float* fparams, void* const* inputs, void* const* outputs, void* stream);
+/* same as _batch through a CUDA graph captured on first use (re-captured when
+ * the arguments change); a repeated _batch call with unchanged arguments
+ * relaunches kernels only */
+int pipeline_pyramid_batch_graph(int n, const int* iparams, const float* fparams, void* const* inputs, void* const* outputs, void* stream);
 /* status of the last call: 0 ok, 1 bad parameters, 2 CUDA error, 3 kernel error */
 int pipeline_pyramid_status(void);
 /* synchronizes and reports the device error word */

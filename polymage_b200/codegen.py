@@ -32,7 +32,10 @@ sandbox/codegen.py:957-1007, sandbox/targetc.py:344-366):
   void* stream)`` -- device buffers, asynchronous on ``stream``.
 * ``int pipeline_<name>_batch(int n, const int* iparams,
   const float* fparams, void* const* in, void* const* out, void* stream)``
-  -- many images (each with its own parameters) in one launch per group.
+  -- many images (each with its own parameters) in one launch per group;
+  when a group has more tiles than fit on the GPU at once, a persistent
+  grid drains a device-side tile queue over all images.
+* ``int pipeline_<name>_batch_graph(...)`` -- the batch as one CUDA graph.
 * ``int pipeline_<name>_graph(params..., ptrs..., void* stream)`` -- replays
   a CUDA graph of the whole pipeline captured on first use.
 * ``int pipeline_<name>_status(void)`` and ``int pipeline_<name>_check(void)``
@@ -784,11 +787,48 @@ class PipelineGen(object):
         w("// Batched execution: n images (each with its own parameters) run")
         w("// through each group in one launch; a CTA maps its block index to")
         w("// (image, tile) through the per-image tile prefix.")
+        w("// A call repeating the previous call's arguments (same images,")
+        w("// parameters and workspace) relaunches the kernels with the")
+        w("// descriptors already on the device: no host copies, so it can be")
+        w("// captured in a CUDA graph (pipeline_<name>_batch_graph).")
+        w("static std::vector<char> pm_batch_key;")
+        w("static void* pm_batch_ws = nullptr;")
+        image_tables = any(img for _, img in self.const_replay)
+        w("// const tables still those the last batch uploaded (a single-image")
+        w("// call in between may have replaced them)")
+        w.open("static bool pm_batch_tables_current()")
+        if image_tables:
+            w("return false;   // a table depends on input image contents")
+        else:
+            for fnm, _ in self.const_replay:
+                w("if (ctab_key_%s != pm_bctab_key_%s || ctab_ptr_%s != "
+                  "pm_bctab_ptr_%s) return false;" % (fnm, fnm, fnm, fnm))
+            w("return true;")
+        w.close()
         w.open('extern "C" int pipeline_%s_batch(int n, const int* iparams, '
                'const float* fparams, void* const* inputs, void* const* '
                'outputs, void* stream)' % name)
         w("cudaStream_t s = (cudaStream_t)stream;")
         w("if (n <= 0) return pm_status = PM_OK;")
+        w("std::vector<char> key;")
+        w("pm_key_add(key, &n, sizeof(n));")
+        w("pm_key_add(key, iparams, sizeof(int) * (size_t)n * %d);" %
+          len(self.iparams))
+        w("pm_key_add(key, fparams, sizeof(float) * (size_t)n * %d);" %
+          len(self.fparams))
+        w("pm_key_add(key, inputs, sizeof(void*) * (size_t)n * %d);" % nin)
+        w("pm_key_add(key, outputs, sizeof(void*) * (size_t)n * %d);" % nout)
+        w("int dev = 0; cudaGetDevice(&dev);")
+        w.open("if (key == pm_batch_key && pm_batch_ws && dev >= 0 && dev < 64"
+               " && pm_batch_arena.ptr[dev] == pm_batch_ws && "
+               "pm_batch_tables_current())")
+        w("int st = 0;")
+        for fnm in self.batch_fns:
+            w("if ((st = %s(nullptr, nullptr, 0, n, nullptr, nullptr, nullptr, "
+              "s, 1))) return pm_status = st;" % fnm)
+        w("return pm_status = PM_OK;")
+        w.close()
+        w("pm_batch_key.clear(); pm_batch_ws = nullptr;")
         w("std::vector<pm_args> As(n);")
         w("std::vector<size_t> wsoffs((size_t)n * %d);" % max(self.nslots, 1))
         w("size_t total = 0;")
@@ -832,8 +872,70 @@ class PipelineGen(object):
         w("size_t doff = 0; int st = 0;")
         for fnm in self.batch_fns:
             w("if ((st = %s(As.data(), wsoffs.data(), %d, n, pm_batch_pinned, "
-              "ddesc, &doff, s))) return pm_status = st;" % (
+              "ddesc, &doff, s, 0))) return pm_status = st;" % (
                   fnm, max(self.nslots, 1)))
+        w("pm_batch_key = key; pm_batch_ws = ws;")
+        w("return pm_status = PM_OK;")
+        w.close()
+        w("")
+        w("static cudaGraphExec_t pm_bgraph_exec = nullptr;")
+        w("static std::vector<char> pm_bgraph_key;")
+        w("static void* pm_bgraph_ws = nullptr;")
+        w("static cudaStream_t pm_bgraph_stream = nullptr;")
+        w("// The batch as one CUDA graph: captured on first use (after one")
+        w("// ordinary call has sized the workspace and uploaded descriptors),")
+        w("// re-captured when the arguments change.")
+        w.open('extern "C" int pipeline_%s_batch_graph(int n, const int* '
+               'iparams, const float* fparams, void* const* inputs, void* '
+               'const* outputs, void* stream)' % name)
+        if image_tables:
+            w("// a const table is computed on the host from input image")
+            w("// contents, which a captured graph would not see change")
+            w("return pm_status = PM_ERR_UNSUPPORTED;")
+            w.close()
+            w("")
+            return
+        w("cudaStream_t s = (cudaStream_t)stream;")
+        w("std::vector<char> key;")
+        w("pm_key_add(key, &n, sizeof(n));")
+        w("pm_key_add(key, iparams, sizeof(int) * (size_t)n * %d);" %
+          len(self.iparams))
+        w("pm_key_add(key, fparams, sizeof(float) * (size_t)n * %d);" %
+          len(self.fparams))
+        w("pm_key_add(key, inputs, sizeof(void*) * (size_t)n * %d);" % nin)
+        w("pm_key_add(key, outputs, sizeof(void*) * (size_t)n * %d);" % nout)
+        w("int dev = 0; cudaGetDevice(&dev);")
+        w("void* wsnow = (dev >= 0 && dev < 64) ? pm_batch_arena.ptr[dev] : "
+          "nullptr;")
+        w.open("if (!pm_bgraph_exec || key != pm_bgraph_key || wsnow != "
+               "pm_bgraph_ws || !pm_batch_tables_current())")
+        w("int st = pipeline_%s_batch(n, iparams, fparams, inputs, outputs, "
+          "stream);" % name)
+        w("if (st) return st;")
+        w("if (cudaStreamSynchronize(s) != cudaSuccess) return pm_status = "
+          "PM_ERR_CUDA;")
+        w("if (!pm_bgraph_stream && cudaStreamCreateWithFlags("
+          "&pm_bgraph_stream, cudaStreamNonBlocking) != cudaSuccess) return "
+          "pm_status = PM_ERR_CUDA;")
+        w("if (pm_bgraph_exec) { cudaGraphExecDestroy(pm_bgraph_exec); "
+          "pm_bgraph_exec = nullptr; }")
+        w("cudaGraph_t g = nullptr;")
+        w("if (cudaStreamBeginCapture(pm_bgraph_stream, "
+          "cudaStreamCaptureModeThreadLocal) != cudaSuccess) return "
+          "pm_status = PM_ERR_CUDA;")
+        w("st = pipeline_%s_batch(n, iparams, fparams, inputs, outputs, "
+          "pm_bgraph_stream);   // replays: kernels only" % name)
+        w("cudaError_t e = cudaStreamEndCapture(pm_bgraph_stream, &g);")
+        w("if (st || e != cudaSuccess) { if (g) cudaGraphDestroy(g); "
+          "cudaGetLastError(); return pm_status = st ? st : PM_ERR_CUDA; }")
+        w("e = cudaGraphInstantiate(&pm_bgraph_exec, g, 0);")
+        w("cudaGraphDestroy(g);")
+        w("if (e != cudaSuccess) { pm_bgraph_exec = nullptr; return "
+          "pm_status = PM_ERR_CUDA; }")
+        w("pm_bgraph_key = key; pm_bgraph_ws = pm_batch_arena.ptr[dev];")
+        w.close()
+        w("if (cudaGraphLaunch(pm_bgraph_exec, s) != cudaSuccess) return "
+          "pm_status = PM_ERR_CUDA;")
         w("return pm_status = PM_OK;")
         w.close()
         w("")
@@ -865,6 +967,14 @@ class PipelineGen(object):
             "device pointers */" % (len(self.inputs), len(self.outputs)),
             "int pipeline_%s_batch(int n, const int* iparams, const float* "
             "fparams, void* const* inputs, void* const* outputs, void* "
+            "stream);" % name,
+            "/* same as _batch through a CUDA graph captured on first use "
+            "(re-captured when",
+            " * the arguments change); a repeated _batch call with unchanged "
+            "arguments",
+            " * relaunches kernels only */",
+            "int pipeline_%s_batch_graph(int n, const int* iparams, const "
+            "float* fparams, void* const* inputs, void* const* outputs, void* "
             "stream);" % name,
             "/* status of the last call: 0 ok, 1 bad parameters, 2 CUDA "
             "error, 3 kernel error */",
@@ -946,6 +1056,8 @@ class StencilGen(object):
         w("%s_desc d0;" % k)
         w("const %s_desc* descs;" % k)
         w("int nimg;")
+        w("int total;           // tiles over all images")
+        w("int* queue;          // tile queue counter (persistent launch)")
         w.close("};")
         w("")
         self.gen_kernel()
@@ -964,7 +1076,21 @@ class StencilGen(object):
           '__grid_constant__ %s_launch L)' % (nt, k, k))
         w.open("")
         w("extern __shared__ __align__(128) unsigned char pm_smem[];")
-        w("const int tile = blockIdx.x;")
+        if self.stage_nodes:
+            # one mbarrier per CTA for the staged inputs, initialized once;
+            # each tile that issues TMA loads completes one phase of it
+            w("uint64_t* pm_bar = reinterpret_cast<uint64_t*>(pm_smem + %d);"
+              % (plan.smem_bytes - 128))
+            w.open("if (threadIdx.x == 0)")
+            w("pm_mbar_init(pm_bar, 1);")
+            w("pm_fence_barrier_init();")
+            w.close()
+            w("__syncthreads();")
+            w("uint32_t pm_phase = 0;")
+        w("__shared__ int pm_next_tile;")
+        w("// Tiles: blockIdx.x first; with a tile queue (persistent launch)")
+        w("// each CTA then takes the next index from the device counter.")
+        w.open("for (int tile = blockIdx.x; tile < L.total; )")
         w("const %s_desc* Dp = &L.d0;" % k)
         w("if (L.nimg > 1) Dp = L.descs + pm_find_image(L.descs, L.nimg, "
           "tile);")
@@ -1005,6 +1131,15 @@ class StencilGen(object):
         self.gen_staging()
         for f in plan.steps:
             self.gen_step(f)
+        w("if (!L.queue) break;")
+        if self.stage_nodes:
+            w("pm_fence_proxy_async();   // the next tile's TMA rewrites smem")
+        w("__syncthreads();      // shared memory is reused by the next tile")
+        w("if (threadIdx.x == 0) pm_next_tile = (int)gridDim.x + "
+          "atomicAdd(L.queue, 1);")
+        w("__syncthreads();")
+        w("tile = pm_next_tile;")
+        w.close()
         w.close()
         w("")
 
@@ -1344,9 +1479,6 @@ class StencilGen(object):
         stage_nodes = self.stage_nodes
         if not stage_nodes:
             return
-        bar_off = plan.smem_bytes - 128
-        w("uint64_t* pm_bar = reinterpret_cast<uint64_t*>(pm_smem + %d);" %
-          bar_off)
         conds = []
         for n in stage_nodes:
             nm = self.node_name(n)
@@ -1354,11 +1486,6 @@ class StencilGen(object):
                 nm, nm, self.empty_expr(n)))
             conds.append("use_tma_%s" % nm)
         w("const bool any_tma = %s;" % " || ".join(conds))
-        w.open("if (any_tma && threadIdx.x == 0)")
-        w("pm_mbar_init(pm_bar, 1);")
-        w("pm_fence_barrier_init();")
-        w.close()
-        w("__syncthreads();")
         w.open("if (any_tma && threadIdx.x == 0)")
         w("uint32_t bytes = 0;")
         for n in stage_nodes:
@@ -1408,7 +1535,8 @@ class StencilGen(object):
             w.close()
             w.close()
         w.open("if (any_tma)")
-        w("pm_mbar_wait(pm_bar, 0, &pm_err_word);")
+        w("pm_mbar_wait(pm_bar, pm_phase, &pm_err_word);")
+        w("pm_phase ^= 1u;")
         w.close()
         w("__syncthreads();")
 
@@ -1667,6 +1795,7 @@ class StencilGen(object):
         w("int st = %s(L.d0, A, wsoff, &nt); if (st) return st;" % fill)
         w("if (nt == 0) return PM_OK;")
         w("if (nt > 0x7fffffffLL) return PM_ERR_UNSUPPORTED;")
+        w("L.total = (int)nt; L.queue = nullptr;")
         w.open("if (!%s_attr)" % k)
         w("if (cudaFuncSetAttribute(%s, cudaFuncAttributeMaxDynamicShared"
           "MemorySize, %d) != cudaSuccess) return PM_ERR_CUDA;" % (
@@ -1679,9 +1808,25 @@ class StencilGen(object):
         w.close()
         w("")
         # batched: descriptors for all images in one upload
+        # The last batch launch is kept so that an unchanged batch can be
+        # replayed (kernels only: descriptors already on the device).
+        w("static %s_launch pm_bl_%s;" % (k, k))
+        w("static long long pm_bgrid_%s = 0;" % k)
+        w("static bool pm_bvalid_%s = false;" % k)
+        w("static int %s_resident = 0;" % k)
         w.open("static int batch_%s(pm_args* As, const size_t* wsoffs, int "
                "nslot, int n, char* pinned, char* ddesc, size_t* doff, "
-               "cudaStream_t s)" % k)
+               "cudaStream_t s, int replay)" % k)
+        w.open("if (replay)")
+        w("if (!pm_bvalid_%s) return PM_ERR_CUDA;" % k)
+        w("if (pm_bgrid_%s == 0) return PM_OK;" % k)
+        w("if (pm_bl_%s.queue && cudaMemsetAsync(pm_bl_%s.queue, 0, "
+          "sizeof(int), s) != cudaSuccess) return PM_ERR_CUDA;" % (k, k))
+        w("%s<<<(unsigned)pm_bgrid_%s, %d, %d, s>>>(pm_bl_%s);" % (
+            k, k, plan.threads, plan.smem_bytes, k))
+        w("return cudaGetLastError() == cudaSuccess ? PM_OK : PM_ERR_CUDA;")
+        w.close()
+        w("pm_bvalid_%s = false;" % k)
         w("size_t off = (*doff + 63) & ~size_t(63);")
         w("%s_desc* H = reinterpret_cast<%s_desc*>(pinned + off);" % (k, k))
         w("long long base = 0;")
@@ -1692,7 +1837,11 @@ class StencilGen(object):
         w("H[i].tile_base = (int)base; base += nt;")
         w.close()
         w("*doff = off + sizeof(%s_desc) * n;" % k)
-        w("if (base == 0) return PM_OK;")
+        w("size_t qoff = (*doff + 63) & ~size_t(63); *doff = qoff + 64;")
+        w.open("if (base == 0)")
+        w("pm_bgrid_%s = 0; pm_bvalid_%s = true;" % (k, k))
+        w("return PM_OK;")
+        w.close()
         w("if (base > 0x7fffffffLL) return PM_ERR_UNSUPPORTED;")
         w("if (cudaMemcpyAsync(ddesc + off, H, sizeof(%s_desc) * n, "
           "cudaMemcpyHostToDevice, s) != cudaSuccess) return PM_ERR_CUDA;" % k)
@@ -1701,13 +1850,32 @@ class StencilGen(object):
         w("L.nimg = n; L.descs = reinterpret_cast<const %s_desc*>(ddesc + "
           "off);" % k)
         w("if (n == 1) L.d0 = H[0];")
+        w("L.total = (int)base;")
         w.open("if (!%s_attr)" % k)
         w("if (cudaFuncSetAttribute(%s, cudaFuncAttributeMaxDynamicShared"
           "MemorySize, %d) != cudaSuccess) return PM_ERR_CUDA;" % (
               k, plan.smem_bytes))
         w("%s_attr = true;" % k)
         w.close()
-        w("%s<<<(unsigned)base, %d, %d, s>>>(L);" % (k, plan.threads,
+        w("// persistent launch: as many CTAs as fit on the GPU at once; they")
+        w("// drain a device-side tile queue spanning every image of the batch")
+        w.open("if (!%s_resident)" % k)
+        w("int per_sm = 0, sms = 0, dev = 0;")
+        w("cudaGetDevice(&dev);")
+        w("cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);")
+        w("cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, %s, %d, %d);"
+          % (k, plan.threads, plan.smem_bytes))
+        w("%s_resident = pm_llmax(1, (long long)per_sm * sms);" % k)
+        w.close()
+        w("long long grid = base;")
+        w.open("if (pm_persistent() && base > %s_resident)" % k)
+        w("L.queue = reinterpret_cast<int*>(ddesc + qoff);")
+        w("if (cudaMemsetAsync(L.queue, 0, sizeof(int), s) != cudaSuccess) "
+          "return PM_ERR_CUDA;")
+        w("grid = %s_resident;" % k)
+        w.close()
+        w("pm_bl_%s = L; pm_bgrid_%s = grid; pm_bvalid_%s = true;" % (k, k, k))
+        w("%s<<<(unsigned)grid, %d, %d, s>>>(L);" % (k, plan.threads,
                                                     plan.smem_bytes))
         w("return cudaGetLastError() == cudaSuccess ? PM_OK : PM_ERR_CUDA;")
         w.close()
@@ -2011,9 +2179,22 @@ class ReductionGen(object):
         w("return cudaGetLastError() == cudaSuccess ? PM_OK : PM_ERR_CUDA;")
         w.close()
         w("")
+        w("static %s_launch pm_bl_%s;" % (k, k))
+        w("static long long pm_bbase_%s = 0, pm_bcells_%s = 0;" % (k, k))
+        w("static bool pm_bvalid_%s = false;" % k)
         w.open("static int batch_%s(pm_args* As, const size_t* wsoffs, int "
                "nslot, int n, char* pinned, char* ddesc, size_t* doff, "
-               "cudaStream_t s)" % k)
+               "cudaStream_t s, int replay)" % k)
+        w.open("if (replay)")
+        w("if (!pm_bvalid_%s) return PM_ERR_CUDA;" % k)
+        w("if (pm_bcells_%s > 0) %s_init<<<(unsigned)pm_llmin((pm_bcells_%s + "
+          "255) / 256, 148LL * 16), 256, 0, s>>>(pm_bl_%s);" % (k, k, k, k))
+        w("if (pm_bbase_%s > 0) %s<<<(unsigned)pm_bbase_%s, %d, %d, s>>>"
+          "(pm_bl_%s);" % (k, k, k, plan.threads, max(plan.smem_bytes, 16),
+                           k))
+        w("return cudaGetLastError() == cudaSuccess ? PM_OK : PM_ERR_CUDA;")
+        w.close()
+        w("pm_bvalid_%s = false;" % k)
         w("size_t off = (*doff + 63) & ~size_t(63);")
         w("%s_desc* H = reinterpret_cast<%s_desc*>(pinned + off);" % (k, k))
         w("long long base = 0, cells = 0;")
@@ -2031,6 +2212,8 @@ class ReductionGen(object):
         w("L.nimg = n; L.descs = reinterpret_cast<const %s_desc*>(ddesc + "
           "off);" % k)
         w("if (n == 1) L.d0 = H[0];")
+        w("pm_bl_%s = L; pm_bbase_%s = base; pm_bcells_%s = cells; "
+          "pm_bvalid_%s = base <= 0x7fffffffLL;" % (k, k, k, k))
         w("if (cells > 0) %s_init<<<(unsigned)pm_llmin((cells + 255) / 256, "
           "148LL * 16), 256, 0, s>>>(L);" % k)
         w("if (base == 0) return cudaGetLastError() == cudaSuccess ? PM_OK : "
@@ -2189,12 +2372,28 @@ class ConstGen(object):
         pg.const_ptrs.append(fnm)
         pg.launch_fns.append("launch_const_" + fnm)
         pg.batch_fns.append("batch_const_" + fnm)
+        # A table computed from input images depends on their contents,
+        # which a replayed batch does not look at: such pipelines never
+        # replay.
+        pg.const_replay.append((fnm, any(isinstance(o, C.Image)
+                                         for o in reads)))
+        w("static std::vector<char> pm_bctab_key_%s;" % fnm)
+        w("static char* pm_bctab_ptr_%s = nullptr;" % fnm)
         w.open("static int batch_const_%s(pm_args* As, const size_t* wsoffs, "
                "int nslot, int n, char* pinned, char* ddesc, size_t* doff, "
-               "cudaStream_t s)" % fnm)
-        w("for (int i = 1; i < n; ++i) if (memcmp(&As[i], &As[0], "
-          "sizeof(pm_args)) != 0) { /* tables depend on parameters only */ }")
-        w("return launch_const_%s(As[0], wsoffs, s);" % fnm)
+               "cudaStream_t s, int replay)" % fnm)
+        w("if (replay) return PM_OK;    // the table is already on the device")
+        w("// one table for the batch: every image must use the same "
+          "parameters")
+        w.open("for (int i = 1; i < n; ++i)")
+        for q in pg.params:
+            w("if (As[i].%s != As[0].%s) return PM_ERR_UNSUPPORTED;" % (
+                pg.pmap[q], pg.pmap[q]))
+        w.close()
+        w("int st = launch_const_%s(As[0], wsoffs, s);" % fnm)
+        w("pm_bctab_key_%s = ctab_key_%s; pm_bctab_ptr_%s = ctab_ptr_%s;" % (
+            fnm, fnm, fnm, fnm))
+        w("return st;")
         w.close()
         w("")
 
@@ -2215,6 +2414,7 @@ def generate_code_for_pipeline(pipeline):
     pg.batch_fns = []
     pg.desc_sizes = []
     pg.const_ptrs = []
+    pg.const_replay = []
     # const tables are addressed through ctab pointers set by their launch
     pg.buf_expr_orig = pg.buf_expr
     body = W()
@@ -2256,6 +2456,11 @@ def generate_code_for_pipeline(pipeline):
     w("static bool pm_use_tma() { static int v = -1; if (v < 0) { const char*"
       " e = getenv(\"PM_DISABLE_TMA\"); v = (e && e[0] == '1') ? 0 : 1; } "
       "return v == 1; }")
+    w("static void pm_key_add(std::vector<char>& k, const void* p, size_t n)"
+      " { if (n) k.insert(k.end(), (const char*)p, (const char*)p + n); }")
+    w("static bool pm_persistent() { static int v = -1; if (v < 0) { const "
+      "char* e = getenv(\"PM_PERSISTENT\"); v = (e && e[0] == '0') ? 0 : 1; }"
+      " return v == 1; }")
     w("static bool pm_host_ptr(const void* p) { cudaPointerAttributes a; if "
       "(cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError();"
       " return true; } return a.type != cudaMemoryTypeDevice && a.type != "
@@ -2267,9 +2472,11 @@ def generate_code_for_pipeline(pipeline):
     pg.gen_validate()
     pg.gen_workspace()
     w.lines.extend(body.lines)
+    # per group: up to 63 B of alignment before its descriptors, then up to
+    # 63 B more and 64 B for its tile-queue counter
     w("static size_t pm_batch_desc_bytes(int n) { return (size_t)n * (%s) + "
-      "64 * %d; }" % (" + ".join(pg.desc_sizes) or "0",
-                      len(pg.desc_sizes) + 1))
+      "192 * %d; }" % (" + ".join(pg.desc_sizes) or "0",
+                       len(pg.desc_sizes) + 1))
     w("")
     pg.gen_entries()
     header = pg.gen_header()

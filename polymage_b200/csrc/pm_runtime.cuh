@@ -71,6 +71,12 @@ __device__ __forceinline__ void pm_fence_barrier_init() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+// order this thread's generic-proxy shared-memory accesses before later
+// async-proxy (TMA) writes to the same bytes
+__device__ __forceinline__ void pm_fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 __device__ __forceinline__ void pm_mbar_arrive_expect_tx(uint64_t* bar,
                                                          uint32_t bytes) {
   asm volatile(

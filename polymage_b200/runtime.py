@@ -55,6 +55,9 @@ class CompiledPipeline(object):
                                 ctypes.c_void_p, ctypes.c_void_p,
                                 ctypes.c_void_p, ctypes.c_void_p]
         self._batch.restype = ctypes.c_int
+        self._batch_graph = getattr(self.lib, "pipeline_%s_batch_graph" % n)
+        self._batch_graph.argtypes = self._batch.argtypes
+        self._batch_graph.restype = ctypes.c_int
         self._status = getattr(self.lib, "pipeline_%s_status" % n)
         self._status.restype = ctypes.c_int
         self._check = getattr(self.lib, "pipeline_%s_check" % n)
@@ -175,9 +178,12 @@ class CompiledPipeline(object):
                 STATUS_TEXT.get(st, st)))
         return outputs
 
-    def run_batch(self, params_list, inputs_list, outputs_list, stream=None):
+    def run_batch(self, params_list, inputs_list, outputs_list, stream=None,
+                  graph=False):
         """Many images in one launch per group; each entry of the lists is a
-        dict as for ``run_dev``."""
+        dict as for ``run_dev``.  ``graph=True`` runs the batch as a CUDA
+        graph (captured on the first call, re-captured when the arguments
+        change)."""
         import torch
         n = len(params_list)
         ip = [p for p in self.params if p.typ not in (C.Float, C.Double)]
@@ -203,11 +209,13 @@ class CompiledPipeline(object):
         outs = np.ascontiguousarray(outs[:, :len(self.outputs)])
         if stream is None:
             stream = torch.cuda.current_stream().cuda_stream
-        st = self._batch(n, iarr.ctypes.data, farr.ctypes.data,
-                         ins.ctypes.data, outs.ctypes.data, stream)
+        fn = self._batch_graph if graph else self._batch
+        st = fn(n, iarr.ctypes.data, farr.ctypes.data, ins.ctypes.data,
+                outs.ctypes.data, stream)
         if st != 0:
-            raise PipelineRuntimeError("pipeline_%s_batch failed: %s" % (
-                self.name, STATUS_TEXT.get(st, st)))
+            raise PipelineRuntimeError("pipeline_%s_batch%s failed: %s" % (
+                self.name, "_graph" if graph else "",
+                STATUS_TEXT.get(st, st)))
         return outputs_list
 
     def check(self):
