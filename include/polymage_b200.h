@@ -24,7 +24,13 @@
  *   int pipeline_<name>_batch(int n, const int* iparams,
  *                             const float* fparams, void* const* inputs,
  *                             void* const* outputs, void* stream);
- *     n images, each with its own parameters, one launch per group.
+ *     n images, each with its own parameters, one launch per group; a
+ *     group with more tiles than fit on the GPU at once runs as a
+ *     persistent grid over a device-side tile queue.  A call repeating
+ *     the previous call's arguments relaunches the kernels only.
+ *
+ *   int pipeline_<name>_batch_graph(same arguments as _batch);
+ *     The batch as one CUDA graph, captured on first use.
  *
  *   int pipeline_<name>_status(void);   status of the last call
  *   int pipeline_<name>_check(void);    synchronizes, reads the device

@@ -44,3 +44,13 @@ def test_every_header_is_covered():
                 for _, b in catalog.default_builds())
     for path in glob.glob(os.path.join(INC, "pipeline_*.h")):
         assert os.path.basename(path) in names
+
+
+def test_costmodel_library_exports_declared_symbols():
+    from polymage_b200 import costmodel
+    lib = costmodel.lib()
+    text = open(os.path.join(INC, "pm_costmodel.h")).read()
+    syms = re.findall(r'^\s*(?:long|int|void)\s+(pm_\w+)\s*\(', text, re.M)
+    assert len(syms) >= 6
+    for s in syms:
+        assert hasattr(lib, s), s
