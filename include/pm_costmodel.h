@@ -34,6 +34,18 @@ int pm_mlp_backward(const float* params, int D, int H, const float* X,
                     const float* y, int B, float* acts, float* work,
                     float* grads, float* loss, void* stream);
 
+/* As pm_mlp_forward, with the activations in a fixed array inside the
+ * library instead of a caller buffer: allocates nothing.  No counterpart in
+ * the reference.  For callers that cannot allocate device memory where they
+ * rank configurations (a fixed device budget, or no cudaMalloc between
+ * timed kernels).  Limit: B * (6 * H + 1) <= 196864 floats (256 rows at
+ * H = 128); larger requests return 1 and launch nothing.  The first call on
+ * each device looks up the array's address (make it before any stream
+ * capture).  Nothing needs to start at zero.  Calls on one device share the
+ * array: two in flight at once race, so issue them on one stream. */
+int pm_mlp_forward_static(const float* params, int D, int H, const float* X,
+                          int B, float* out, void* stream);
+
 /* one Adam step (t: 1-based step number) */
 int pm_mlp_adam(float* params, const float* grads, float* m, float* v, int D,
                 int H, int t, float lr, float weight_decay, void* stream);

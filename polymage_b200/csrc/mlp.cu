@@ -181,3 +181,70 @@ int pm_mlp_adam(float* params, const float* grads, float* m, float* v, int D,
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Inference that allocates nothing: pm_mlp_forward_static.
+//
+// pm_mlp_forward takes its activation buffer from the caller.  Some callers
+// cannot allocate device memory at the point where they rank configurations:
+// a host runtime that hands out a fixed device budget reserved at start-up,
+// or a tuning loop that must not add a cudaMalloc (which can synchronize the
+// whole device) between the kernels it is timing.  This entry keeps the
+// activations in a fixed array of this module instead.  It runs the same
+// kernels as pm_mlp_forward, in the same order.
+//
+// Limit: B * (6 * H + 1) floats of activations, at most
+// PM_MLP_STATIC_FLOATS = 196,864 floats (787,456 bytes; 256 rows at H = 128).
+// A larger request returns 1 and launches nothing.
+// Set-up: the first call on each device looks up the array's device address
+// with that device current; make that first call before any stream capture.
+// Initial contents: nothing in the array needs to start at zero; every float
+// the kernels read was written earlier in the same call.
+// Concurrency: all calls on one device share the array, so two calls in
+// flight at once (on different streams, or from different host threads
+// without ordering) race on it; issue them on one stream.
+#include <mutex>
+
+#define PM_MLP_STATIC_FLOATS 196864
+#define PM_MLP_STATIC_DEVICES 64
+
+namespace {
+
+__device__ __align__(256) float pm_mlp_static_acts[PM_MLP_STATIC_FLOATS];
+
+float* pm_mlp_static_ptr[PM_MLP_STATIC_DEVICES];
+std::mutex pm_mlp_static_mu;
+
+// device address of the array on the current device (looked up once)
+float* static_acts(int dev) {
+  std::lock_guard<std::mutex> lk(pm_mlp_static_mu);
+  if (!pm_mlp_static_ptr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, pm_mlp_static_acts) != cudaSuccess)
+      return nullptr;
+    pm_mlp_static_ptr[dev] = static_cast<float*>(p);
+  }
+  return pm_mlp_static_ptr[dev];
+}
+
+}  // namespace
+
+extern "C" int pm_mlp_forward_static(const float* params, int D, int H,
+                                     const float* X, int B, float* out,
+                                     void* stream) {
+  if (D <= 0 || H <= 0 || B < 0) return 1;
+  if ((long long)B * (6LL * H + 1) > PM_MLP_STATIC_FLOATS) return 1;
+  if (B == 0) return 0;
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 ||
+      dev >= PM_MLP_STATIC_DEVICES)
+    return 2;
+  float* acts = static_acts(dev);
+  if (!acts) return 2;
+  cudaStream_t s = (cudaStream_t)stream;
+  forward(params, D, H, X, B, acts, s);
+  if (cudaMemcpyAsync(out, acts + (size_t)B * 6 * H, sizeof(float) * B,
+                      cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+    return 2;
+  return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
