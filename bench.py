@@ -16,6 +16,9 @@ Reported (one JSON line, rank 0):
   cpu_baseline  the reference's own generated C++ (pipeline_mask, OpenMP on
             all host cores) on a bounded sample of the same workload
   clocks    SM clocks and throttle reasons sampled during the timed region
+  pipelines every shipped pipeline (Harris, unsharp, camera pipe, bilateral
+            grid, pyramid blending) at its benchmark size: MPix/s and the
+            compulsory-bytes HBM roofline fraction (polymage_b200.apps.measure)
 
 ``--impl reference`` times the reference's CPU implementation alone.
 Multi-GPU (torchrun): every rank runs its own image (replicas, weak
@@ -309,6 +312,14 @@ def run(args):
             "gpu_launches": args.steps,
             "clocks": clk,
         }
+        if not args.no_pipelines:
+            # every shipped pipeline at its benchmark size (device buffers,
+            # L2 flushed before each run): MPix/s and compulsory-bytes
+            # roofline fraction
+            from polymage_b200.apps import measure
+            line["pipelines"] = dict(
+                (a, measure.measure(a, steps=50, warmup=5, device=dev))
+                for a in measure.APPS)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line))
@@ -326,6 +337,8 @@ def main():
     ap.add_argument("--impl", default="polymage_b200",
                     choices=["polymage_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-pipelines", action="store_true",
+                    help="skip the per-pipeline throughput table")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

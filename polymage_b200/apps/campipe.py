@@ -20,6 +20,15 @@ from ..constructs import (Parameter, Variable, Interval, Image, Function,
                           Float, Short, UChar)
 from ..compiler import buildPipeline
 
+# The app's colour-correction matrices at 3200 K and 7000 K (campipe/
+# init.py:26-40), rows r, g, b of [3x3 | offset]: benchmark inputs.
+MATRIX_3200 = ((1.6697, -0.2693, -0.4004, -42.4346),
+               (-0.3576, 1.0615, 1.5949, -37.1158),
+               (-0.2175, -1.8751, 6.9640, -26.6970))
+MATRIX_7000 = ((2.2997, -0.4478, 0.1706, -39.0923),
+               (-0.3826, 1.5906, -0.2080, -25.4311),
+               (-0.0888, -0.7344, 2.2832, -20.0826))
+
 
 def camera_pipe(pipe_data=None):
     x = Variable(Int, "x")

@@ -1,5 +1,7 @@
-"""The pipelines this backend ships prebuilt, with their default settings
-(tile sizes and register blocking chosen by measurement on B200)."""
+"""The pipelines this backend ships prebuilt, with their default settings:
+the best of exhaustive tuning on B200 at each pipeline's benchmark size
+(15 tile shapes x 5 group sizes x register blocking 2/4/8, five timed runs
+each; polymage_b200.autotune)."""
 
 import functools
 
@@ -9,12 +11,12 @@ from .campipe import build_campipe
 from .bilateral_grid import build_bilateral
 from .pyramid_blend import build_pyramid
 
-HARRIS = dict(tile_sizes=(32, 64), options=('rblock=4',))
-UNSHARP = dict(tile_sizes=(32, 128), options=('rblock=8',))
-CAMPIPE = dict(tile_sizes=(32, 128), group_size=5, options=('rblock=4',))
-BILATERAL = dict(tile_sizes=(1, 32, 64), group_size=5,
+HARRIS = dict(tile_sizes=(32, 64), group_size=10, options=('rblock=8',))
+UNSHARP = dict(tile_sizes=(32, 128), group_size=10, options=('rblock=8',))
+CAMPIPE = dict(tile_sizes=(32, 64), group_size=9, options=('rblock=8',))
+BILATERAL = dict(tile_sizes=(1, 32, 128), group_size=7,
                  options=(('red_tile', (32, 256)), 'rblock=4'))
-PYRAMID = dict(tile_sizes=(16, 128), group_size=10, options=('rblock=4',))
+PYRAMID = dict(tile_sizes=(32, 64), group_size=10, options=('rblock=8',))
 
 _BUILDERS = {
     "harris": (build_harris, HARRIS),

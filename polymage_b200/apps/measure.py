@@ -1,0 +1,130 @@
+"""Throughput of the shipped pipelines at their benchmark sizes on the GPU.
+
+  python -m polymage_b200.apps.measure --app harris --steps 50 --warmup 5
+
+For each pipeline: synthetic inputs of the benchmark size (seeded), the
+default build from the catalog, device buffers, and ``--steps`` timed runs
+of the whole pipeline (every group's launch) through ``pipeline_<name>_dev``.
+Before each timed run a 256 MB buffer is written so that no input is still
+in the 126 MB L2; each run is bracketed by CUDA events on the launching
+stream.  Reported per pipeline: mean pipeline time, MPix/s (pixels of the
+benchmark image), and the compulsory-bytes roofline: (input bytes + output
+bytes) / time against the measured HBM copy bandwidth.
+"""
+
+import argparse
+import json
+import os
+
+import numpy as np
+
+from . import catalog
+
+APPS = ("harris", "unsharp", "campipe", "bilateral", "pyramid")
+FLUSH_BYTES = 256 << 20
+
+
+def workload(app, seed=0):
+    """(params, host inputs, output shapes/dtypes, pixels, description)."""
+    rng = np.random.default_rng(seed)
+    if app == 'harris':
+        n = 2048
+        return ({'R': n - 2, 'C': n - 2},
+                {'img': rng.random((n, n), dtype=np.float32)},
+                {'harris': ((n, n), np.float32)}, n * n,
+                "harris 2048x2048 float32")
+    if app == 'unsharp':
+        n = 4096
+        img = np.zeros((3, n + 4, n + 4), np.float32)
+        img[:, 2:n + 2, 2:n + 2] = rng.random((3, n, n), dtype=np.float32)
+        return ({'R': n, 'C': n, 'threshold': 0.001, 'weight': 3.0},
+                {'img': img}, {'mask': ((3, n, n), np.float32)}, n * n,
+                "unsharp_mask 3x4096x4096 float32")
+    if app == 'campipe':
+        R, C = 1968, 2592
+        from .campipe import MATRIX_3200, MATRIX_7000
+        return ({'R': R, 'C': C, 'colour_temp': 3700.0, 'contrast': 50.0,
+                 'gamma': 2.0},
+                {'img': rng.integers(0, 1024, (R, C), dtype=np.int16),
+                 'matrix_3200': np.asarray(MATRIX_3200, np.float32),
+                 'matrix_7000': np.asarray(MATRIX_7000, np.float32)},
+                {'process': ((3, R - 48, C - 64), np.uint8)}, R * C,
+                "camera_pipe 2592x1968 uint16 raw -> uint8 RGB")
+    if app == 'bilateral':
+        rows, cols = 1536, 2560
+        return ({'rows': rows, 'cols': cols},
+                {'input': rng.random((rows, cols), dtype=np.float32)},
+                {'filtered': ((1, rows, cols), np.float32)}, rows * cols,
+                "bilateral_grid 2560x1536 float32")
+    if app == 'pyramid':
+        R = C = 2108
+        return ({'R': R, 'C': C},
+                {'img1': rng.random((3, R, C), dtype=np.float32),
+                 'img2': rng.random((3, R, C), dtype=np.float32),
+                 'mask': rng.random((R, C), dtype=np.float32)},
+                {'blend': ((3, R - 60, C - 60), np.float32)}, R * C,
+                "pyramid_blend L=4 3x2108x2108 float32")
+    raise ValueError(app)
+
+
+def hbm_peak():
+    root = os.path.dirname(os.path.dirname(os.path.dirname(
+        os.path.abspath(__file__))))
+    p = os.path.join(root, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def measure(app, steps=50, warmup=5, device=None):
+    import torch
+    dev = device or torch.device("cuda", torch.cuda.current_device())
+    cp = catalog.build(app)
+    prm, host_in, out_spec, pixels, desc = workload(app)
+    ins = dict((k, torch.from_numpy(v).to(dev)) for k, v in host_in.items())
+    outs = {}
+    for k, (shape, dt) in out_spec.items():
+        outs[k] = torch.zeros(shape, dtype=torch.from_numpy(
+            np.zeros(1, dt)).dtype, device=dev)
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(max(warmup, 3)):
+        cp.run_dev(prm, ins, outs, stream=stream.cuda_stream)
+    torch.cuda.synchronize(dev)
+    cp.check()
+    ev = [(torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for i in range(steps):
+        flush.fill_(float(i))
+        ev[i][0].record(stream)
+        cp.run_dev(prm, ins, outs, stream=stream.cuda_stream)
+        ev[i][1].record(stream)
+    torch.cuda.synchronize(dev)
+    cp.check()
+    ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
+    nbytes = sum(v.nbytes for v in host_in.values()) + sum(
+        int(np.prod(s)) * np.dtype(d).itemsize for s, d in out_spec.values())
+    peak, kind = hbm_peak()
+    gbs = nbytes / (ms / 1e3) / 1e9
+    return {"app": app, "workload": desc, "ms": ms,
+            "mpix_s": pixels / (ms / 1e3) / 1e6,
+            "launches": sum({'stencil': 1, 'reduction': 2}.get(g['kind'], 0)
+                            for g in cp.module.meta.get('groups', [])),
+            "compulsory_bytes": int(nbytes), "achieved_gbs": gbs,
+            "hbm_frac": gbs / peak, "peak_gbs": peak, "peak_source": kind,
+            "l2": "256 MB written before each timed run"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--app", action="append", choices=APPS)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    args = ap.parse_args()
+    for app in args.app or APPS:
+        print(json.dumps(measure(app, args.steps, args.warmup)))
+
+
+if __name__ == "__main__":
+    main()

@@ -21,7 +21,7 @@ import numpy as np
 from . import tuner
 from .apps.harris import harris_pipe
 from .apps.unsharp_mask import unsharp_mask
-from .apps.campipe import camera_pipe
+from .apps.campipe import camera_pipe, MATRIX_3200, MATRIX_7000
 from .apps.bilateral_grid import bilateral_grid
 from .apps.pyramid_blend import pyramid_blending
 from .constructs import Condition
@@ -49,12 +49,8 @@ def app_setup(app, seed=0):
         out = camera_pipe(d)
         R, C = 1968, 2592
         est = [(d['R'], R), (d['C'], C)]
-        m3 = np.array([[1.6697, -0.2693, -0.4004, -42.4346],
-                       [-0.3576, 1.0615, 1.5949, -37.1158],
-                       [-0.2175, -1.8751, 6.9640, -26.6970]], np.float32)
-        m7 = np.array([[2.2997, -0.4478, 0.1706, -39.0923],
-                       [-0.3826, 1.5906, -0.2080, -25.4311],
-                       [-0.0888, -0.7344, 2.2832, -20.0826]], np.float32)
+        m3 = np.array(MATRIX_3200, np.float32)
+        m7 = np.array(MATRIX_7000, np.float32)
         data = {'C': C, 'R': R, 'colour_temp': 3700.0, 'contrast': 50.0,
                 'gamma': 2.0,
                 'img': rng.integers(0, 1024, (R, C), dtype=np.int16),
