@@ -628,6 +628,19 @@ class PipelineGen(object):
         w("static pm_arena pm_host_in[%d];" % max(nin, 1))
         w("static pm_arena pm_host_out[%d];" % max(nout, 1))
         w("static cudaStream_t pm_host_stream[64];")
+        if self.band_group() is not None:
+            w("// row-band overlap of copies and compute (host entry)")
+            w("#define PM_MAX_BANDS 128")
+            w("static cudaStream_t pm_band_in[64], pm_band_out[64];")
+            w("static cudaEvent_t pm_band_ev[64][PM_MAX_BANDS * 2 + 1];")
+            w("static bool pm_band_ready[64];")
+            w("// bands to aim for: PM_HOST_BANDS (0 disables banding), else 12")
+            w.open("static int pm_target_bands()")
+            w("static int v = -1;")
+            w("if (v < 0) { const char* e = getenv(\"PM_HOST_BANDS\"); "
+              "v = e ? atoi(e) : 12; if (v < 0) v = 0; if (v > 64) v = 64; }")
+            w("return v;")
+            w.close()
         w.open('extern "C" void pipeline_%s(%s)' % (name, sig))
         w("pm_args A; memset(&A, 0, sizeof(A));")
         for line in call_fill:
@@ -651,6 +664,9 @@ class PipelineGen(object):
             w("void* dv_%s = nullptr;" % n)
             w("if (pm_arena_get(&%s, nb_%s, &dv_%s)) { pm_status = "
               "PM_ERR_CUDA; return; }" % (arena, n, n))
+        sg = self.band_group()
+        if sg is not None:
+            self.gen_banded(sg, ctx)
         for f in self.inputs:
             n = self.fn(f)
             w("if (nb_%s && cudaMemcpyAsync(dv_%s, %s, nb_%s, "
@@ -678,6 +694,152 @@ class PipelineGen(object):
         w("pm_status = kerr ? PM_ERR_KERNEL : PM_OK;")
         w.close()
         w("")
+
+    def band_group(self):
+        """The stencil group of a pipeline that the host entry can run in
+        row bands: the pipeline is that one group (no reductions, no const
+        tables), its anchor is the pipeline's only output, and the output's
+        written points form a box."""
+        if len(self.launch_fns) != 1 or len(self.band_groups) != 1 or \
+                len(self.outputs) != 1 or self.const_ptrs:
+            return None
+        sg = self.band_groups[0]
+        out = self.outputs[0]
+        if sg.plan.anchor is not out or out.ndims < 2 or \
+                self.written_box(out) is None:
+            return None
+        return sg
+
+    def gen_banded(self, sg, ctx):
+        """Host buffers in pinned memory: split the tile grid into row bands
+        and overlap, on three streams, the input copy of the next band, the
+        kernel on this band and the output copy of the previous band.  A
+        band's input need is the prefix of each input up to the largest
+        offset its corner tiles read (footprints are monotone in the tile
+        coordinates); its output copy is the written box clipped to the
+        band's anchor region."""
+        w = self.w
+        k = sg.k
+        plan = sg.plan
+        na = plan.anchor.ndims
+        nin = len(self.inputs)
+        out = self.outputs[0]
+        w("bool pm_band = pm_target_bands() > 0 && (%s) >= ((size_t)16 << 20);" %
+          " + ".join("nb_%s" % self.fn(f) for f in self.inputs + self.outputs))
+        w.open("if (pm_band)")
+        w("cudaPointerAttributes pa;")
+        for f in self.inputs + self.outputs:
+            w("if (cudaPointerGetAttributes(&pa, %s) != cudaSuccess || pa.type "
+              "!= cudaMemoryTypeHost) { pm_band = false; cudaGetLastError(); }"
+              % f.name)
+        w.close()
+        w("%s_launch L; memset(&L, 0, sizeof(L));" % k)
+        w("L.nimg = 1;")
+        w("long long nt = 0, nrow = 0, ninner = 0, nouter = 0;")
+        w.open("if (pm_band)")
+        for f in self.inputs + self.outputs:
+            n = self.fn(f)
+            w("A.b_%s = dv_%s;" % (n, n))
+        w("size_t wsoff[%d + 1]; size_t wstotal = 0;" % max(self.nslots, 1))
+        w("pm_ws_layout(A, wsoff, &wstotal);")
+        w("void* ws = nullptr;")
+        w("if (pm_arena_get(&pm_ws_arena, wstotal, &ws)) { pm_status = "
+          "PM_ERR_CUDA; return; }")
+        w("A.ws = (char*)ws;")
+        w("if ((st = fill_%s(L.d0, A, wsoff, &nt))) { pm_status = st; return; }"
+          % k)
+        w("nrow = L.d0.gn[%d]; ninner = L.d0.gn[%d];" % (na - 2, na - 1))
+        w("nouter = (nrow && ninner) ? nt / (nrow * ninner) : 0;")
+        w("if (nt == 0 || nt > 0x7fffffffLL || nouter > 40) pm_band = false;")
+        w.close()
+        w.open("if (pm_band)")
+        w("const %s_desc& D = L.d0;" % k)
+        w.open("if (!pm_band_ready[dev])")
+        w("if (cudaStreamCreateWithFlags(&pm_band_in[dev], "
+          "cudaStreamNonBlocking) != cudaSuccess || cudaStreamCreateWithFlags("
+          "&pm_band_out[dev], cudaStreamNonBlocking) != cudaSuccess) "
+          "{ pm_status = PM_ERR_CUDA; return; }")
+        w("for (int i = 0; i < PM_MAX_BANDS * 2 + 1; ++i) if (cudaEventCreate"
+          "WithFlags(&pm_band_ev[dev][i], cudaEventDisableTiming) != "
+          "cudaSuccess) { pm_status = PM_ERR_CUDA; return; }")
+        w("pm_band_ready[dev] = true;")
+        w.close()
+        w("cudaStream_t sin = pm_band_in[dev], sout = pm_band_out[dev];")
+        w.open("if (!%s_attr)" % k)
+        w("if (cudaFuncSetAttribute(%s, cudaFuncAttributeMaxDynamicShared"
+          "MemorySize, %d) != cudaSuccess) { pm_status = PM_ERR_CUDA; "
+          "return; }" % (k, plan.smem_bytes))
+        w("%s_attr = true;" % k)
+        w.close()
+        w("// the kernel's first band must not start before earlier work on s")
+        w("cudaEventRecord(pm_band_ev[dev][PM_MAX_BANDS * 2], s);")
+        w("cudaStreamWaitEvent(sin, pm_band_ev[dev][PM_MAX_BANDS * 2], 0);")
+        w("cudaStreamWaitEvent(sout, pm_band_ev[dev][PM_MAX_BANDS * 2], 0);")
+        w("long long rb = (nrow * nouter + pm_target_bands() - 1) / "
+          "pm_target_bands();")
+        w("if (rb < 1) rb = 1;")
+        w("if (rb > nrow) rb = nrow;")
+        w("size_t copied[%d] = {0};" % max(nin, 1))
+        w("int bi = 0;")
+        w.open("for (long long o = 0; o < nouter; ++o)")
+        w.open("for (long long a = 0; a < nrow; a += rb)")
+        w("const long long b = a + rb < nrow ? a + rb : nrow;")
+        w("const long long tf = (o * nrow + a) * ninner, tl = (o * nrow + b) "
+          "* ninner;")
+        w("long long need[%d] = {0};" % max(nin, 1))
+        w("int blo[%d], bhi[%d];" % (na, na))
+        w("for (int d = 0; d < %d; ++d) { blo[d] = 0x3fffffff; bhi[d] = "
+          "-0x3fffffff; }" % na)
+        w("const long long corner[4] = {tf, tf + ninner - 1, tl - ninner, "
+          "tl - 1};")
+        w.open("for (int c = 0; c < 4; ++c)")
+        w("long long e[%d]; int alo[%d], ahi[%d];" % (max(nin, 1), na, na))
+        w("%s_footprint(D, (int)corner[c], e, alo, ahi);" % k)
+        w("for (int j = 0; j < %d; ++j) if (e[j] > need[j]) need[j] = e[j];"
+          % nin)
+        w("for (int d = 0; d < %d; ++d) { blo[d] = pm_imin(blo[d], alo[d]); "
+          "bhi[d] = pm_imax(bhi[d], ahi[d]); }" % na)
+        w.close()
+        for j, f in enumerate(self.inputs):
+            n = self.fn(f)
+            w.open("")
+            w("size_t nb = (size_t)need[%d] * %d;" % (j, f.typ.size()))
+            w("if (nb > nb_%s) nb = nb_%s;" % (n, n))
+            w("if (nb > copied[%d] && cudaMemcpyAsync((char*)dv_%s + copied[%d],"
+              " (const char*)%s + copied[%d], nb - copied[%d], "
+              "cudaMemcpyHostToDevice, sin) != cudaSuccess) { pm_status = "
+              "PM_ERR_CUDA; return; }" % (j, n, j, f.name, j, j))
+            w("if (nb > copied[%d]) copied[%d] = nb;" % (j, j))
+            w.close()
+        w("if (bi >= PM_MAX_BANDS) { cudaStreamSynchronize(s); pm_status = "
+          "PM_ERR_UNSUPPORTED; return; }")
+        w("cudaEvent_t ein = pm_band_ev[dev][2 * bi], ek = "
+          "pm_band_ev[dev][2 * bi + 1];")
+        w("if (cudaEventRecord(ein, sin) != cudaSuccess || "
+          "cudaStreamWaitEvent(s, ein, 0) != cudaSuccess) { pm_status = "
+          "PM_ERR_CUDA; return; }")
+        w("L.first = (int)tf; L.total = (int)tl; L.queue = nullptr;")
+        w("%s<<<(unsigned)(tl - tf), %d, %d, s>>>(L);" % (k, plan.threads,
+                                                         plan.smem_bytes))
+        w("if (cudaGetLastError() != cudaSuccess || cudaEventRecord(ek, s) != "
+          "cudaSuccess || cudaStreamWaitEvent(sout, ek, 0) != cudaSuccess) "
+          "{ pm_status = PM_ERR_CUDA; return; }")
+        clip = [("blo[%d]" % d, "bhi[%d]" % d) for d in range(na)]
+        self.gen_d2h(out, ctx, stream="sout",
+                     fail="{ pm_status = PM_ERR_CUDA; return; }", clip=clip)
+        w("++bi;")
+        w.close()
+        w.close()
+        w("if (cudaEventRecord(pm_band_ev[dev][PM_MAX_BANDS * 2], sout) != "
+          "cudaSuccess || cudaStreamWaitEvent(s, pm_band_ev[dev][PM_MAX_BANDS "
+          "* 2], 0) != cudaSuccess) { pm_status = PM_ERR_CUDA; return; }")
+        w("if (cudaStreamSynchronize(s) != cudaSuccess) { pm_status = "
+          "PM_ERR_CUDA; return; }")
+        w("unsigned kerr = 0;")
+        w("cudaMemcpyFromSymbol(&kerr, pm_err_word, sizeof(kerr));")
+        w("pm_status = kerr ? PM_ERR_KERNEL : PM_OK;")
+        w("return;")
+        w.close()
 
     def written_box(self, f):
         """Per-dim (lo, hi) expressions of the points of output ``f`` that
@@ -724,15 +886,19 @@ class PipelineGen(object):
             out.append((lo, hi))
         return out
 
-    def gen_d2h(self, f, ctx):
+    def gen_d2h(self, f, ctx, stream="s",
+                fail="{ pm_status = PM_ERR_CUDA; return; }", clip=None):
+        """Copy the written points of output ``f`` back to the caller's
+        buffer (one 2-D copy per outer index); ``clip`` optionally
+        intersects the written box with per-dim (lo, hi) C expressions."""
         w = self.w
         n = self.fn(f)
         box = self.written_box(f)
         es = f.typ.size()
         if box is None:
             w("if (nb_%s && cudaMemcpyAsync(%s, dv_%s, nb_%s, "
-              "cudaMemcpyDeviceToHost, s) != cudaSuccess) { pm_status = "
-              "PM_ERR_CUDA; return; }" % (n, f.name, n, n))
+              "cudaMemcpyDeviceToHost, %s) != cudaSuccess) %s" % (
+                  n, f.name, n, n, stream, fail))
             return
         nd = len(f.domain)
         w.open("")
@@ -740,9 +906,12 @@ class PipelineGen(object):
             w("const long long D%d_lo = %s, D%d_hi = %s;" % (
                 d, ctx.expr(dom.lowerBound, {}), d,
                 ctx.expr(dom.upperBound, {})))
-            w("const long long B%d_lo = pm_llmax(D%d_lo, %s), B%d_hi = "
-              "pm_llmin(D%d_hi, %s);" % (d, d, ctx.expr(box[d][0], {}), d, d,
-                                         ctx.expr(box[d][1], {})))
+            lo = "pm_llmax(D%d_lo, %s)" % (d, ctx.expr(box[d][0], {}))
+            hi = "pm_llmin(D%d_hi, %s)" % (d, ctx.expr(box[d][1], {}))
+            if clip is not None:
+                lo = "pm_llmax(%s, (long long)(%s))" % (lo, clip[d][0])
+                hi = "pm_llmin(%s, (long long)(%s))" % (hi, clip[d][1])
+            w("const long long B%d_lo = %s, B%d_hi = %s;" % (d, lo, d, hi))
         w("bool nonempty = %s;" % " && ".join(
             "B%d_lo <= B%d_hi" % (d, d) for d in range(nd)))
         w("long long S%d = 1;" % (nd - 1))
@@ -753,9 +922,8 @@ class PipelineGen(object):
         if nd == 1:
             w("size_t o = (size_t)(B0_lo - D0_lo) * %d;" % es)
             w("if (cudaMemcpyAsync((char*)%s + o, (char*)dv_%s + o, "
-              "(size_t)(B0_hi - B0_lo + 1) * %d, cudaMemcpyDeviceToHost, s) "
-              "!= cudaSuccess) { pm_status = PM_ERR_CUDA; return; }" % (
-                  f.name, n, es))
+              "(size_t)(B0_hi - B0_lo + 1) * %d, cudaMemcpyDeviceToHost, %s) "
+              "!= cudaSuccess) %s" % (f.name, n, es, stream, fail))
         else:
             # loops over the outer dims, one 2-D copy per outer point
             for d in range(nd - 2):
@@ -769,9 +937,8 @@ class PipelineGen(object):
             w("size_t pitch = (size_t)S%d * %d;" % (a, es))
             w("if (cudaMemcpy2DAsync((char*)%s + o, pitch, (char*)dv_%s + o, "
               "pitch, (size_t)(B%d_hi - B%d_lo + 1) * %d, (size_t)(B%d_hi - "
-              "B%d_lo + 1), cudaMemcpyDeviceToHost, s) != cudaSuccess) "
-              "{ pm_status = PM_ERR_CUDA; return; }" % (f.name, n, b, b, es,
-                                                         a, a))
+              "B%d_lo + 1), cudaMemcpyDeviceToHost, %s) != cudaSuccess) %s" % (
+                  f.name, n, b, b, es, a, a, stream, fail))
             for d in range(nd - 2):
                 w.close()
         w.close()
@@ -1056,12 +1223,81 @@ class StencilGen(object):
         w("%s_desc d0;" % k)
         w("const %s_desc* descs;" % k)
         w("int nimg;")
+        w("int first;           // tiles [first, total) of this launch")
         w("int total;           // tiles over all images")
         w("int* queue;          // tile queue counter (persistent launch)")
         w.close("};")
         w("")
         self.gen_kernel()
         self.gen_launcher()
+        self.gen_footprint()
+
+    def gen_footprint(self):
+        """Host function ``<k>_footprint(D, tile, in_end, a_lo, a_hi)``: the
+        same region inference as the kernel, for one tile, reduced to what
+        the banded host entry needs: per pipeline input, one past the
+        largest element offset the tile reads (0 when it reads none), and
+        the tile's anchor region."""
+        pg = self.pg
+        plan = self.plan
+        k = self.k
+        na = plan.anchor.ndims
+        saved_w, saved_ctx = pg.w, getattr(self, 'ctx', None)
+        saved_inside = self.has_inside
+        w = W()
+        pg.w = w
+        self.ctx = ExprCtx(w, 'device', pg.pmap, None)
+        w.open("static void %s_footprint(const %s_desc& D, int tile, "
+               "long long* in_end, int* a_lo, int* a_hi)" % (k, k))
+        pg.declare_params(w, "D")
+        w("int rem = tile - D.tile_base;")
+        for d in range(na - 1, 0, -1):
+            w("const int t%d = rem %% D.gn[%d]; rem /= D.gn[%d];" % (d, d, d))
+        w("const int t0 = rem;")
+        for d in range(na):
+            w("const int a_lo%d = D.glo[%d] + t%d * %d;" % (d, d, d,
+                                                           plan.tile[d]))
+            w("const int a_hi%d = pm_imin(a_lo%d + %d, D.ghi[%d]);" % (
+                d, d, plan.tile[d] - 1, d))
+        seen = set()
+        for n in plan.nodes:
+            if id(n.func) not in seen:
+                seen.add(id(n.func))
+                pg.declare_domain(w, n.func, self.ctx, False)
+        self.gen_regions()
+        w("(void)t0;")
+        for j, f in enumerate(pg.inputs):
+            w("in_end[%d] = 0;" % j)
+            n = plan.node_of.get(f)
+            if n is None or n.role not in ('stage', 'global'):
+                continue
+            nm = self.node_name(n)
+            fnm = pg.fn(f)
+            nd = n.ndims
+            w.open("")
+            empty = []
+            for d in range(nd):
+                w("const int h%d = pm_imin(r_%s_hi%d, d_%s_hi%d), l%d = "
+                  "pm_imax(r_%s_lo%d, d_%s_lo%d);" % (d, nm, d, fnm, d, d, nm,
+                                                      d, fnm, d))
+                empty.append("l%d > h%d" % (d, d))
+            w("long long o = 0, s = 1;")
+            for d in range(nd - 1, -1, -1):
+                w("o += (long long)(h%d - d_%s_lo%d) * s; s *= (long long)"
+                  "(d_%s_hi%d - d_%s_lo%d + 1);" % (d, fnm, d, fnm, d, fnm, d))
+            w("if (!(%s)) in_end[%d] = o + 1;" % (" || ".join(empty), j))
+            w.close()
+        an = self.node_name(plan.node_of[plan.anchor])
+        for d in range(na):
+            w("a_lo[%d] = r_%s_lo%d; a_hi[%d] = r_%s_hi%d;" % (d, an, d, d, an,
+                                                              d))
+        w.close()
+        w("")
+        pg.w = saved_w
+        self.ctx = saved_ctx
+        self.has_inside = saved_inside
+        pg.w.lines.extend(w.lines)
+        pg.band_groups.append(self)
 
     # ---- kernel -------------------------------------------------------------
     def gen_kernel(self):
@@ -1090,7 +1326,7 @@ class StencilGen(object):
         w("__shared__ int pm_next_tile;")
         w("// Tiles: blockIdx.x first; with a tile queue (persistent launch)")
         w("// each CTA then takes the next index from the device counter.")
-        w.open("for (int tile = blockIdx.x; tile < L.total; )")
+        w.open("for (int tile = L.first + (int)blockIdx.x; tile < L.total; )")
         w("const %s_desc* Dp = &L.d0;" % k)
         w("if (L.nimg > 1) Dp = L.descs + pm_find_image(L.descs, L.nimg, "
           "tile);")
@@ -1135,7 +1371,7 @@ class StencilGen(object):
         if self.stage_nodes:
             w("pm_fence_proxy_async();   // the next tile's TMA rewrites smem")
         w("__syncthreads();      // shared memory is reused by the next tile")
-        w("if (threadIdx.x == 0) pm_next_tile = (int)gridDim.x + "
+        w("if (threadIdx.x == 0) pm_next_tile = L.first + (int)gridDim.x + "
           "atomicAdd(L.queue, 1);")
         w("__syncthreads();")
         w("tile = pm_next_tile;")
@@ -2412,6 +2648,7 @@ def generate_code_for_pipeline(pipeline):
     pg.nslots = len(getattr(pipeline, '_storage_slots', []))
     pg.launch_fns = []
     pg.batch_fns = []
+    pg.band_groups = []
     pg.desc_sizes = []
     pg.const_ptrs = []
     pg.const_replay = []

@@ -37,9 +37,9 @@
 // ---------------------------------------------------------------------------
 // device helpers
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int pm_imin(int a, int b) { return a < b ? a : b; }
-__device__ __forceinline__ int pm_imax(int a, int b) { return a > b ? a : b; }
-__device__ __forceinline__ int pm_clampi(int v, int lo, int hi) {
+__host__ __device__ __forceinline__ int pm_imin(int a, int b) { return a < b ? a : b; }
+__host__ __device__ __forceinline__ int pm_imax(int a, int b) { return a > b ? a : b; }
+__host__ __device__ __forceinline__ int pm_clampi(int v, int lo, int hi) {
   return v < lo ? lo : (v > hi ? hi : v);
 }
 __host__ __device__ __forceinline__ int pm_floordiv(int a, int b) {
