@@ -62,6 +62,22 @@ def _dist():
     return ws, rank
 
 
+def max_over_ranks(x, device, world_size):
+    """The largest of every rank's ``x`` (a time), for whole-job rates."""
+    if world_size <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank, world_size, seconds):
+    """Whole-job throughput: every rank processed ``units_per_rank``."""
+    return world_size * units_per_rank / seconds
+
+
 # ---------------------------------------------------------------------------
 class Clocks(object):
     """nvidia-smi sampler running while the timed region runs."""
@@ -254,11 +270,8 @@ def run(args):
     cp.check()
     elapsed_ms = t0.elapsed_time(t1)
     kern_ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
-    if ws > 1:
-        t = torch.tensor([elapsed_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
-    value = ws * args.steps * R * C / (elapsed_ms / 1e3) / 1e6
+    elapsed_ms = max_over_ranks(elapsed_ms, dev, ws)
+    value = job_rate(args.steps * R * C, ws, elapsed_ms / 1e3) / 1e6
 
     # --- end to end through the reference C ABI (host buffers) -------------
     pin_in = torch.empty(host_in.shape, dtype=torch.float32,
@@ -275,11 +288,8 @@ def run(args):
     for _ in range(e2e_steps):
         cp.run_host(prm, {'img': a_in}, {'mask': a_out})
     e2e_s = time.perf_counter() - s0
-    if ws > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = ws * e2e_steps * R * C / e2e_s / 1e6
+    e2e_s = max_over_ranks(e2e_s, dev, ws)
+    e2e = job_rate(e2e_steps * R * C, ws, e2e_s) / 1e6
 
     if rank == 0:
         peak, peak_kind = _peaks()

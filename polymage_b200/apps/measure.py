@@ -7,9 +7,9 @@ default build from the catalog, device buffers, and ``--steps`` timed runs
 of the whole pipeline (every group's launch) through ``pipeline_<name>_dev``.
 Before each timed run a 256 MB buffer is written so that no input is still
 in the 126 MB L2; each run is bracketed by CUDA events on the launching
-stream.  Reported per pipeline: mean pipeline time, MPix/s (pixels of the
-benchmark image), and the compulsory-bytes roofline: (input bytes + output
-bytes) / time against the measured HBM copy bandwidth.
+stream.  Reported per pipeline: mean pipeline time, MPix/s (spatial pixels
+of the output, rows x cols), and the compulsory-bytes roofline: (input
+bytes + output bytes) / time against the measured HBM copy bandwidth.
 """
 
 import argparse
@@ -48,7 +48,8 @@ def workload(app, seed=0):
                 {'img': rng.integers(0, 1024, (R, C), dtype=np.int16),
                  'matrix_3200': np.asarray(MATRIX_3200, np.float32),
                  'matrix_7000': np.asarray(MATRIX_7000, np.float32)},
-                {'process': ((3, R - 48, C - 64), np.uint8)}, R * C,
+                {'process': ((3, R - 48, C - 64), np.uint8)},
+                (R - 48) * (C - 64),
                 "camera_pipe 2592x1968 uint16 raw -> uint8 RGB")
     if app == 'bilateral':
         rows, cols = 1536, 2560
@@ -62,7 +63,8 @@ def workload(app, seed=0):
                 {'img1': rng.random((3, R, C), dtype=np.float32),
                  'img2': rng.random((3, R, C), dtype=np.float32),
                  'mask': rng.random((R, C), dtype=np.float32)},
-                {'blend': ((3, R - 60, C - 60), np.float32)}, R * C,
+                {'blend': ((3, R - 60, C - 60), np.float32)},
+                (R - 60) * (C - 60),
                 "pyramid_blend L=4 3x2108x2108 float32")
     raise ValueError(app)
 

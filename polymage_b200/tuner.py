@@ -170,9 +170,25 @@ def pipeline_features(pipe):
 
 
 # ---------------------------------------------------------------------------
+_flush_buf = None
+
+
+def _flush_l2(stream):
+    """Write a 256 MB buffer (twice the 126 MB L2) so that a timed run
+    starts with none of its inputs or intermediates cached."""
+    global _flush_buf
+    import torch
+    if _flush_buf is None:
+        _flush_buf = torch.empty(64 << 20, dtype=torch.float32,
+                                 device=torch.cuda.current_device())
+    with torch.cuda.stream(stream):
+        _flush_buf.fill_(0.0)
+
+
 def _time_config(so_path, pipe_name, params, dev_inputs, dev_outputs, nruns,
                  warmup=2):
-    """min-of-nruns device time (ms) of one compiled configuration."""
+    """min-of-nruns device time (ms) of one compiled configuration, L2
+    flushed before every timed run."""
     import ctypes
     import torch
     from . import constructs as C
@@ -208,6 +224,7 @@ def _time_config(so_path, pipe_name, params, dev_inputs, dev_outputs, nruns,
     for _ in range(nruns):
         s = torch.cuda.Event(enable_timing=True)
         e = torch.cuda.Event(enable_timing=True)
+        _flush_l2(stream)
         s.record(stream)
         fn(*args)
         e.record(stream)
