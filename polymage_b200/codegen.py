@@ -160,6 +160,9 @@ class ExprCtx(object):
         self.reader = reader
         self.scopes = [{}]
         self.ntemp = 0
+        # lower bounds of loop variables (C name -> int), for emitting
+        # unsigned division/modulo where the numerator cannot be negative
+        self.var_lo = {}
 
     def temp(self):
         self.ntemp += 1
@@ -222,6 +225,12 @@ class ExprCtx(object):
             args = [_subst(a, bind) for a in e.arguments]
             return self.reader(e.objectRef, args, self)
         if isinstance(e, AbstractBinaryOpNode):
+            if e.op in ('/', '%') and self._unsigned_ok(e, bind):
+                # truncating division of a non-negative int by a positive
+                # constant equals unsigned division (a shift or mask for
+                # powers of two); C semantics are unchanged
+                return "((int)((unsigned)(%s) %s %du))" % (
+                    self.expr(e.left, bind), e.op, int(e.right.value))
             return "(%s %s %s)" % (self.expr(e.left, bind), e.op,
                                    self.expr(e.right, bind))
         if isinstance(e, AbstractUnaryOpNode):
@@ -249,6 +258,29 @@ class ExprCtx(object):
         return {C.Pow: 'pow', C.Powf: 'powf', C.Log: 'log', C.Exp: 'exp',
                 C.Sin: 'sin', C.Cos: 'cos', C.Sqrt: 'sqrt', C.Sqrtf: 'sqrtf',
                 C.Abs: 'pm_abs'}[type(e)]
+
+    def _unsigned_ok(self, e, bind):
+        if not self.var_lo:
+            return False
+        r = e.right
+        if not (isinstance(r, Value) and r.typ in _INT_T and r.typ is not
+                C.Long and r.typ is not C.ULong and int(r.value) > 0):
+            return False
+        try:
+            if getType(e.left) is not C.Int:
+                return False
+        except Exception:
+            return False
+        f = affine_form(_subst(e.left, bind))
+        if f is None:
+            return False
+        low = f[1]
+        for v, c in f[0].items():
+            lo = self.var_lo.get(getattr(v, '_cname', None))
+            if lo is None or c < 0:
+                return False
+            low += c * lo
+        return low >= 0
 
     def cond(self, c, bind):
         op = c.conditional
@@ -296,6 +328,17 @@ def _subst(a, bind):
     if not m:
         return a
     return substitute_vars(a, m)
+
+
+def _const_int(e):
+    """The value of an integer constant expression, else None."""
+    try:
+        f = affine_form(e)
+    except Exception:
+        return None
+    if f is None or f[0]:
+        return None
+    return int(f[1])
 
 
 def _loop_vars(n, prefix="q"):
@@ -1896,18 +1939,29 @@ class StencilGen(object):
         inner = ext[-1]
         if nd >= 2:
             outer = ext[-2]
-            K = 1
-            for k in (8, 4, 2, 1):
-                if k <= rb_max and outer % k == 0:
-                    K = k
-                    break
+            # block height: fewest rows loaded (block + a 2-row halo) per
+            # row computed; a last partial block is shifted back to end at
+            # the last row (its overlap is recomputed, same values)
+            K, best = 1, None
+            for k in range(min(rb_max, outer), 0, -1):
+                cost = -(-outer // k) * (k + 2)
+                if best is None or cost < best:
+                    K, best = k, cost
         else:
             outer, K = 1, 1
-        nblk = outer // K
+        # a small outermost dimension (channels) is computed by the same
+        # thread, so that reads and index arithmetic shared by the channels
+        # of a point are done once
+        cb = 1
+        if nd >= 3 and ext[0] <= 4 and 'no_cblock' not in pg.p.options:
+            cb = ext[0]
+            while K > 1 and K * cb > 16:
+                K -= 1
+        nblk = -(-outer // K)
         rest = ext[:-2] if nd >= 2 else []
         total = nblk * inner
-        for e in rest:
-            total *= e
+        for d, e in enumerate(rest):
+            total *= 1 if (d == 0 and cb > 1) else e
         strides = []
         st = 1
         for e in reversed(ext):
@@ -1917,10 +1971,15 @@ class StencilGen(object):
             total, plan.threads))
         w("const int ji = it %% %d; int rr = it / %d;" % (inner, inner))
         if nd >= 2:
-            w("const int jo = (rr %% %d) * %d; rr /= %d;" % (nblk, K, nblk))
+            if outer % K:
+                w("const int jo = pm_imin((rr %% %d) * %d, %d); rr /= %d;" % (
+                    nblk, K, outer - K, nblk))
+            else:
+                w("const int jo = (rr %% %d) * %d; rr /= %d;" % (nblk, K,
+                                                                nblk))
         for d in range(len(rest) - 1, -1, -1):
             if d == 0:
-                w("const int j%d = rr;" % d)
+                w("const int j0 = %s;" % ("0" if cb > 1 else "rr"))
             else:
                 w("const int j%d = rr %% %d; rr /= %d;" % (d, rest[d],
                                                           rest[d]))
@@ -1943,27 +2002,43 @@ class StencilGen(object):
                 for d in range(nd)))
         ctx = self.ctx
         ctx.push()
+        saved_lo = dict(ctx.var_lo)
+        for d, dom in enumerate(f.domain):
+            lo = _const_int(dom.lowerBound)
+            if lo is not None:
+                # regions are clamped to the domain: qb >= its lower bound
+                ctx.var_lo["qb%d" % d] = lo
         flagged = n.role == 'out' and comp.is_output
-        for k in range(K):
-            pt = list(base)
-            qs = ["qb%d" % d for d in range(nd)]
-            if nd >= 2 and k:
-                pt[nd - 2] = base[nd - 2] + k
-                qs[nd - 2] = "(qb%d + %d)" % (nd - 2, k)
-            bind = dict(zip(f.variables, pt))
-            v = "v%d" % k
-            w("%s %s = 0;" % (ctype(f.typ), v))
-            flag = None
-            if flagged:
-                flag = "wr%d" % k
-                w("bool %s = false;" % flag)
-            self.emit_cases(f, bind, v, flag)
-            idx = "ib" if k == 0 else "ib + %d" % (k * strides[nd - 2])
-            gidx = None
-            if n.role == 'out':
-                gidx = "gb" if k == 0 else "gb + %d * s_%s_%d" % (
-                    k, fnm, nd - 2)
-            self._store(f, n, qs, v, flag, idx, gidx)
+        for c in range(cb):
+            for k in range(K):
+                pt = list(base)
+                qs = ["qb%d" % d for d in range(nd)]
+                if nd >= 2 and k:
+                    pt[nd - 2] = base[nd - 2] + k
+                    qs[nd - 2] = "(qb%d + %d)" % (nd - 2, k)
+                if c:
+                    pt[0] = base[0] + c
+                    qs[0] = "(qb0 + %d)" % c
+                bind = dict(zip(f.variables, pt))
+                v = "v%d_%d" % (c, k)
+                w("%s %s = 0;" % (ctype(f.typ), v))
+                flag = None
+                if flagged:
+                    flag = "wr%d_%d" % (c, k)
+                    w("bool %s = false;" % flag)
+                self.emit_cases(f, bind, v, flag)
+                off = k * strides[nd - 2] + c * strides[0]
+                idx = "ib" if off == 0 else "ib + %d" % off
+                gidx = None
+                if n.role == 'out':
+                    terms = ["gb"]
+                    if k:
+                        terms.append("%d * s_%s_%d" % (k, fnm, nd - 2))
+                    if c:
+                        terms.append("%d * s_%s_0" % (c, fnm))
+                    gidx = " + ".join(terms)
+                self._store(f, n, qs, v, flag, idx, gidx)
+        ctx.var_lo = saved_lo
         ctx.pop()
         w.close()
 
