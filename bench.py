@@ -330,6 +330,8 @@ def run(args):
             line["pipelines"] = dict(
                 (a, measure.measure(a, steps=50, warmup=5, device=dev))
                 for a in measure.APPS)
+            line["pipelines"]["bilateral_batch64"] = \
+                measure.measure_bilateral_batch(64, device=dev)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line))

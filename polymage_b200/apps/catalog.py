@@ -11,7 +11,7 @@ from .campipe import build_campipe
 from .bilateral_grid import build_bilateral
 from .pyramid_blend import build_pyramid
 
-HARRIS = dict(tile_sizes=(32, 64), group_size=10, options=('rblock=8',))
+HARRIS = dict(tile_sizes=(16, 128), group_size=11, options=('rblock=8',))
 UNSHARP = dict(tile_sizes=(32, 128), group_size=10, options=('rblock=8',))
 CAMPIPE = dict(tile_sizes=(32, 64), group_size=9, options=('rblock=8',))
 BILATERAL = dict(tile_sizes=(1, 32, 128), group_size=7,

@@ -118,14 +118,71 @@ def measure(app, steps=50, warmup=5, device=None):
             "l2": "256 MB written before each timed run"}
 
 
+def measure_bilateral_batch(n=64, steps=10, warmup=3, graph=True,
+                            device=None, seed=1):
+    """The batched bilateral-grid workload: ``n`` images whose sides are
+    drawn uniformly from 512..4096 (seeded), each U[0,1), run as one batch
+    (one launch per group, persistent tile queue) through
+    ``pipeline_bilateral_batch_graph`` (or ``_batch``).  Inputs are created
+    on the device; timed with CUDA events, L2 flushed before each run."""
+    import torch
+    dev = device or torch.device("cuda", torch.cuda.current_device())
+    cp = catalog.build("bilateral")
+    rng = np.random.default_rng(seed)
+    sides = rng.integers(512, 4097, (n, 2))
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    prms, ins, outs = [], [], []
+    for r, c in sides:
+        r, c = int(r), int(c)
+        prms.append({'rows': r, 'cols': c})
+        ins.append({'input': torch.rand((r, c), generator=gen, device=dev)})
+        outs.append({'filtered': torch.zeros((1, r, c), device=dev)})
+    pixels = float(sum(int(r) * int(c) for r, c in sides))
+    nbytes = pixels * 8
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(max(warmup, 3)):
+        cp.run_batch(prms, ins, outs, stream=stream.cuda_stream, graph=graph)
+    torch.cuda.synchronize(dev)
+    cp.check()
+    ev = [(torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for i in range(steps):
+        flush.fill_(float(i))
+        ev[i][0].record(stream)
+        cp.run_batch(prms, ins, outs, stream=stream.cuda_stream, graph=graph)
+        ev[i][1].record(stream)
+    torch.cuda.synchronize(dev)
+    cp.check()
+    ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
+    peak, kind = hbm_peak()
+    gbs = nbytes / (ms / 1e3) / 1e9
+    return {"app": "bilateral_batch%d" % n,
+            "workload": "bilateral_grid batch of %d images, sides "
+                        "U{512..4096} seed %d, %.1f MPix" % (n, seed,
+                                                             pixels / 1e6),
+            "ms": ms, "mpix_s": pixels / (ms / 1e3) / 1e6,
+            "entry": "pipeline_bilateral_batch_graph" if graph
+            else "pipeline_bilateral_batch",
+            "compulsory_bytes": int(nbytes), "achieved_gbs": gbs,
+            "hbm_frac": gbs / peak, "peak_gbs": peak, "peak_source": kind,
+            "l2": "256 MB written before each timed run"}
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--app", action="append", choices=APPS)
+    ap.add_argument("--app", action="append",
+                    choices=APPS + ("bilateral_batch64",))
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     args = ap.parse_args()
-    for app in args.app or APPS:
-        print(json.dumps(measure(app, args.steps, args.warmup)))
+    for app in args.app or APPS + ("bilateral_batch64",):
+        if app == "bilateral_batch64":
+            print(json.dumps(measure_bilateral_batch(
+                64, steps=min(args.steps, 10), warmup=args.warmup)))
+        else:
+            print(json.dumps(measure(app, args.steps, args.warmup)))
 
 
 if __name__ == "__main__":

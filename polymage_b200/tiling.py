@@ -670,6 +670,29 @@ def infer_regions(plan, anchor_box, env, clamp=True, tile_first=None):
     return regions
 
 
+def _grid_lo(plan):
+    """Per anchor dim, the first tile origin when it is a constant (the
+    smallest lower bound of the live-outs' domains along that dim, as the
+    generated descriptor filler computes it), else None."""
+    from .codegen import _const_int
+    na = plan.anchor.ndims
+    out = [None] * na
+    seen = [False] * na
+    ok = [True] * na
+    for n in plan.nodes:
+        if n.role != 'out' and n.func is not plan.anchor:
+            continue
+        for d, dom in enumerate(n.func.domain):
+            k = d if n.func is plan.anchor else n.owned_map[d]
+            v = _const_int(dom.lowerBound)
+            if v is None:
+                ok[k] = False
+                continue
+            out[k] = v if not seen[k] else min(out[k], v)
+            seen[k] = True
+    return [out[k] if ok[k] and seen[k] else None for k in range(na)]
+
+
 def _static_extents(plan, env):
     # period of every node's region in the tile origin: the lcm, over the
     # chains of uses from the anchor, of the product of the divisors met
@@ -699,14 +722,21 @@ def _static_extents(plan, env):
     plan.period = period
     exts = []
     adom = _domain_vals(plan.anchor, env)
+    glo = _grid_lo(plan)
     for base in (period * (1 << 22), period * (1 << 23) + period * 7):
         # anchor dims of constant extent: their actual tiles; parametric
-        # dims: every residue of the origin, far from any border
+        # dims: the residues of the origin (mod the period) that tiles can
+        # have, far from any border -- all of them unless the tile grid
+        # starts at a constant, when only glo + j*tile occur
         axes = []
         for k, t in enumerate(plan.tile):
             if _const_extent(plan.anchor.domain[k], env) is not None:
                 lo0, hi0 = adom[k]
                 axes.append(np.arange(lo0, hi0 + 1, t, dtype=np.int64))
+            elif glo[k] is not None:
+                res = sorted(set((glo[k] + j * t) % period
+                                 for j in range(period)))
+                axes.append(base + np.asarray(res, dtype=np.int64))
             else:
                 axes.append(base + np.arange(period, dtype=np.int64))
         grids = np.meshgrid(*axes, indexing='ij')
