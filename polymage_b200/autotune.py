@@ -7,8 +7,9 @@ Exhaustive mode runs ``tuner.generate`` + ``tuner.execute`` over the
 reference's search space (15 tile shapes x 5 group sizes, as the
 reference's app tuners use: harris/app_tuner.py:33-54) times the register
 blocking options, appending every measurement to the timing database.
-Learned mode ranks the same space with a trained cost model and times only
-its top-k.
+Learned mode ranks the same space with the cost model (pretrained on the
+other pipelines' measurements) and compiles and times only its top picks,
+in one round.
 """
 
 import argparse
@@ -117,11 +118,15 @@ def main():
                     help='online learned tuning (cost model)')
     ap.add_argument('--compare', action='store_true',
                     help='learned tuning, then exhaustive tuning as judge')
-    ap.add_argument('--rounds', type=int, default=3)
-    ap.add_argument('--batch', type=int, default=2)
+    ap.add_argument('--picks', type=int, default=10,
+                    help='configurations the learned tuner times (one '
+                         'compile round)')
     ap.add_argument('--options', default=None,
                     help='JSON list of option lists to search over')
     ap.add_argument('--report', default=None)
+    ap.add_argument('--train-db', default=None,
+                    help='timing database the learned tuner pretrains on '
+                         '(other pipelines\' rows; default: the shipped one)')
     args = ap.parse_args()
     opts = json.loads(args.options) if args.options else None
     out = {'app': args.app}
@@ -132,8 +137,9 @@ def main():
             a['_tuner_option_configs'] = opts
         a['_tuner_dst_path'] = os.path.join(args.dst, 'learned')
         a['_tuner_nruns'] = args.nruns
-        lr = learned_tune(a, batches=(args.batch * 2, args.batch),
-                          local=args.batch, shipped_app=args.app)
+        rows = tuner.load_db(args.train_db) if args.train_db else None
+        lr = learned_tune(a, db_rows=rows, batches=(args.picks,), local=0,
+                          shipped_app=args.app)
         out['learned'] = {'best': lr['best'], 'best_ms': lr['best_ms'],
                           'wall_s': lr['wall_s'], 'plan_s': lr['plan_s'],
                           'measured': len(lr['measured']),
