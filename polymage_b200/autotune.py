@@ -118,7 +118,7 @@ def main():
                     help='online learned tuning (cost model)')
     ap.add_argument('--compare', action='store_true',
                     help='learned tuning, then exhaustive tuning as judge')
-    ap.add_argument('--picks', type=int, default=10,
+    ap.add_argument('--picks', type=int, default=14,
                     help='configurations the learned tuner times (one '
                          'compile round)')
     ap.add_argument('--options', default=None,

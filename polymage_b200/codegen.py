@@ -330,6 +330,34 @@ def _subst(a, bind):
     return substitute_vars(a, m)
 
 
+def tbind_of(f, rvars, red, rbind):
+    """Binding for a reduction part: reduction variables to the loop
+    variables, and every other function variable to the part's target
+    index (a condition on it restricts the target cell)."""
+    tb = dict(rbind)
+    for fv, ta in zip(f.variables, red.accumulate_ref.arguments):
+        if all(fv is not rv for rv in rvars):
+            tb[fv] = _subst(ta, rbind)
+    return tb
+
+
+def _cond_const_true(c, bind):
+    """True when condition ``c`` holds whatever the loop variables are
+    (after substituting ``bind``; e.g. ``c == 0`` with c bound to 0)."""
+    from .evaluate import try_eval_int
+    op = c.conditional
+    if op == '&&':
+        return _cond_const_true(c.lhs, bind) and _cond_const_true(c.rhs, bind)
+    if op == '||':
+        return _cond_const_true(c.lhs, bind) or _cond_const_true(c.rhs, bind)
+    a = try_eval_int(_subst(c.lhs, bind), {})
+    b = try_eval_int(_subst(c.rhs, bind), {})
+    if a is None or b is None:
+        return False
+    return {'==': a == b, '!=': a != b, '<': a < b, '<=': a <= b,
+            '>': a > b, '>=': a >= b}.get(op, False)
+
+
 def _const_int(e):
     """The value of an integer constant expression, else None."""
     try:
@@ -2353,34 +2381,46 @@ class ReductionGen(object):
         w("if (%s) continue;" % " || ".join("q%d > a_hi%d" % (d, d)
                                            for d in range(nr)))
         rbind = dict(zip(rvars, lv))
-        for cond, expr, red in parts:
-            ctx.push()
+        saved_lo = dict(ctx.var_lo)
+        for d, dom in enumerate(f.reductionDomain):
+            lo = _const_int(dom.lowerBound)
+            if lo is not None:
+                # tiles start at the reduction domain's lower bound
+                ctx.var_lo["q%d" % d] = lo
+        for pi, (cond, expr, red) in enumerate(parts):
+            tbind = tbind_of(f, rvars, red, rbind)
+            # Parts whose condition holds everywhere read in bounds at every
+            # point of the reduction domain (checked per call), so they
+            # share one scope: values they have in common (e.g. an input
+            # pixel) are read once.
+            shared = cond is None or _cond_const_true(cond, tbind)
+            if not shared:
+                ctx.push()
+                w.open("")
             tgt = red.accumulate_ref.arguments
-            tbind = dict(rbind)
-            # a condition on a function variable that is not a reduction
-            # variable restricts the target cell: bind it to the target index
-            for fv, ta in zip(f.variables, tgt):
-                if all(fv is not rv for rv in rvars):
-                    tbind[fv] = _subst(ta, rbind)
-            w.open("")
+            cn = ["c%d_%d" % (d, pi) for d in range(nd)]
             for d, ta in enumerate(tgt):
-                w("const int c%d = %s;" % (d, ctx.expr(ta, rbind)))
-            inb = " && ".join("c%d >= d_%s_lo%d && c%d <= d_%s_hi%d" % (
-                d, fnm, d, d, fnm, d) for d in range(nd))
+                w("const int %s = %s;" % (cn[d], ctx.expr(ta, rbind)))
+            inb = " && ".join("%s >= d_%s_lo%d && %s <= d_%s_hi%d" % (
+                cn[d], fnm, d, cn[d], fnm, d) for d in range(nd))
             cc = ctx.cond(cond, tbind) if cond is not None else "true"
+            val = ctx.expr(expr, rbind) if shared else None
             w.open("if ((%s) && (%s))" % (inb, cc))
-            val = ctx.expr(expr, rbind)
+            if val is None:
+                val = ctx.expr(expr, rbind)
             if priv:
-                sidx = " + ".join("(c%d - p_lo%d) * %d" % (
-                    d, d, _stride(plan.priv_ext, d)) for d in range(nd))
+                sidx = " + ".join("(%s - p_lo%d) * %d" % (
+                    cn[d], d, _stride(plan.priv_ext, d)) for d in range(nd))
                 w("%s(&acc[%s], (%s)(%s));" % (self.atomic(), sidx, T, val))
             else:
-                gidx = " + ".join("(long long)(c%d - d_%s_lo%d) * s_%s_%d" % (
-                    d, fnm, d, fnm, d) for d in range(nd))
+                gidx = " + ".join("(long long)(%s - d_%s_lo%d) * s_%s_%d" % (
+                    cn[d], fnm, d, fnm, d) for d in range(nd))
                 w("%s(&out[%s], (%s)(%s));" % (self.atomic(), gidx, T, val))
             w.close()
-            w.close()
-            ctx.pop()
+            if not shared:
+                w.close()
+                ctx.pop()
+        ctx.var_lo = saved_lo
         w.close()
         if priv:
             w("__syncthreads();")

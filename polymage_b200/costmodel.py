@@ -338,7 +338,7 @@ class OnlineRanker(object):
             pred += m.predict(self.Xc)
         return [int(i) for i in np.argsort(pred)]
 
-    def run(self, cands, measure, batches=(10,), local=0):
+    def run(self, cands, measure, batches=(14,), local=0):
         for b in batches:
             pick = [i for i in self.order() if i not in self.measured][:b]
             if not pick:
@@ -356,7 +356,7 @@ class OnlineRanker(object):
         return min(ok, key=lambda i: self.measured[i]) if ok else None
 
 
-def learned_tune(arg_data, db_rows=None, batches=(10,), local=0,
+def learned_tune(arg_data, db_rows=None, batches=(14,), local=0,
                  ensemble=3, seed=0, shipped_app=None, measure=None):
     """Online learned tuning of one pipeline: plan every configuration of
     the search space (no compilation), keep one per distinct plan, then
@@ -416,7 +416,7 @@ def learned_tune(arg_data, db_rows=None, batches=(10,), local=0,
             'wall_s': time.time() - t0}
 
 
-def evaluate_on_db(rows, app, batches=(10,), local=0, ensemble=3, seed=0):
+def evaluate_on_db(rows, app, batches=(14,), local=0, ensemble=3, seed=0):
     """Replay ``learned_tune`` on recorded measurements of ``app``: the
     ranker only learns the times of the configurations it picks.  Returns
     (best picked ms / best recorded ms, number measured, distinct plans)."""
