@@ -1573,7 +1573,13 @@ class StencilGen(object):
             if len(parts) == 1 and parts[0][0] is None:
                 continue
             if len(parts) != 1:
-                return None
+                # several box-shaped Cases (e.g. one per channel): evaluated
+                # per point by a branch chain in the interior path
+                boxes = part_boxes(f)
+                if len(boxes) != len(parts) or \
+                        not all(b[0].exact for b in boxes):
+                    return None
+                continue
             boxes = part_boxes(f)
             if len(boxes) != 1 or not boxes[0][0].exact:
                 return None
@@ -1744,14 +1750,14 @@ class StencilGen(object):
             if written_flag:
                 w("%s = true;" % written_flag)
             return
-        if self.inside:
+        if self.inside and len(parts) == 1:
             # the single Case holds on the whole region of this tile
             e = ctx.expr(parts[0][1], bind)
             w("%s = (%s)(%s);" % (target, ctype(f.typ), e))
             if written_flag:
                 w("%s = true;" % written_flag)
             return
-        if self.fast:
+        if self.fast and not self.inside:
             # unguarded: every case evaluated, later cases take precedence
             T = ctype(f.typ)
             val = "(%s)0" % T
