@@ -4,7 +4,8 @@
 
 For each pipeline: synthetic inputs of the benchmark size (seeded), the
 default build from the catalog, device buffers, and ``--steps`` timed runs
-of the whole pipeline (every group's launch) through ``pipeline_<name>_dev``.
+of the whole pipeline (every group's launch) through ``pipeline_<name>_graph``
+(the pipeline's kernels as one CUDA graph; ``graph=False``: ``_dev``).
 Before each timed run a 256 MB buffer is written so that no input is still
 in the 126 MB L2; each run is bracketed by CUDA events on the launching
 stream.  Reported per pipeline: mean pipeline time, MPix/s (spatial pixels
@@ -79,7 +80,7 @@ def hbm_peak():
     return 6650.0, "fallback"
 
 
-def measure(app, steps=50, warmup=5, device=None):
+def measure(app, steps=50, warmup=5, device=None, graph=True):
     import torch
     dev = device or torch.device("cuda", torch.cuda.current_device())
     cp = catalog.build(app)
@@ -91,8 +92,15 @@ def measure(app, steps=50, warmup=5, device=None):
             np.zeros(1, dt)).dtype, device=dev)
     flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
+    if graph:
+        from ..runtime import PipelineRuntimeError
+        try:
+            cp.run_dev(prm, ins, outs, stream=stream.cuda_stream, graph=True)
+        except PipelineRuntimeError:
+            # no graph form (const tables computed from input contents)
+            graph = False
     for _ in range(max(warmup, 3)):
-        cp.run_dev(prm, ins, outs, stream=stream.cuda_stream)
+        cp.run_dev(prm, ins, outs, stream=stream.cuda_stream, graph=graph)
     torch.cuda.synchronize(dev)
     cp.check()
     ev = [(torch.cuda.Event(enable_timing=True),
@@ -100,7 +108,7 @@ def measure(app, steps=50, warmup=5, device=None):
     for i in range(steps):
         flush.fill_(float(i))
         ev[i][0].record(stream)
-        cp.run_dev(prm, ins, outs, stream=stream.cuda_stream)
+        cp.run_dev(prm, ins, outs, stream=stream.cuda_stream, graph=graph)
         ev[i][1].record(stream)
     torch.cuda.synchronize(dev)
     cp.check()
@@ -113,6 +121,7 @@ def measure(app, steps=50, warmup=5, device=None):
             "mpix_s": pixels / (ms / 1e3) / 1e6,
             "launches": sum({'stencil': 1, 'reduction': 2}.get(g['kind'], 0)
                             for g in cp.module.meta.get('groups', [])),
+            "entry": "pipeline_%s_%s" % (cp.name, "graph" if graph else "dev"),
             "compulsory_bytes": int(nbytes), "achieved_gbs": gbs,
             "hbm_frac": gbs / peak, "peak_gbs": peak, "peak_source": kind,
             "l2": "256 MB written before each timed run"}

@@ -632,6 +632,18 @@ class PipelineGen(object):
         w("// (re)captured when the arguments or the workspace change.")
         w.open('extern "C" int pipeline_%s_graph(%s, void* stream)' % (name,
                                                                       sig))
+        if any(img for _, img in self.const_replay):
+            w("// a const table is computed on the host from input image")
+            w("// contents, which a captured graph would not see change")
+            for q in self.params:
+                w("(void)%s;" % q.name)
+            for f in self.inputs + self.outputs:
+                w("(void)%s;" % f.name)
+            w("(void)stream;")
+            w("return pm_status = PM_ERR_UNSUPPORTED;")
+            w.close()
+            w("")
+            return self._gen_entries_tail(sig, call_fill)
         w("pm_args A; memset(&A, 0, sizeof(A));")
         for line in call_fill:
             w(line)
@@ -672,6 +684,11 @@ class PipelineGen(object):
         w("return pm_status = PM_OK;")
         w.close()
         w("")
+        self._gen_entries_tail(sig, call_fill)
+
+    def _gen_entries_tail(self, sig, call_fill):
+        w = self.w
+        name = self.pname
         # ---- host pointers (the reference's ABI) ----
         self.gen_host_entry(sig, call_fill)
         # ---- batch ----
