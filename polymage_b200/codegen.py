@@ -55,6 +55,8 @@ as in the reference.
 
 import re
 
+import numpy as np
+
 from . import constructs as C
 from .expr_ast import (Value, AbstractBinaryOpNode, AbstractUnaryOpNode,
                        InbuiltFunction)
@@ -1257,6 +1259,8 @@ class StencilGen(object):
         self.g = group
         self.plan = group.plan
         self.k = "pm_%s_g%d" % (pg.pname, group.level_time)
+        self.vec = 1                  # points per thread along the inner dim
+        self.vec_stats = None
 
     def node_name(self, n):
         return self.pg.fn(n.func)
@@ -1673,6 +1677,8 @@ class StencilGen(object):
         nm = self.node_name(n)
         fnm = self.pg.fn(n.func)
         ext = list(n.ext)
+        if n.role != 'stage' and n.pad_inner:
+            ext[-1] = n.pad_inner
         if n.role == 'stage':
             es = n.func.typ.size()
             al = max(1, 16 // es)
@@ -1725,6 +1731,14 @@ class StencilGen(object):
         w = pg.w
         node = plan.node_of.get(f)
         t = ctx.temp()
+        if node is not None and node.in_smem and self.vec > 1 and \
+                self.inside:
+            vt = self.vec_read(node, f, args)
+            if self.vec_stats is not None:
+                self.vec_stats[0 if vt else 1] += 1
+            if vt is not None:
+                ctx.define(key, vt)
+                return vt
         if node is not None and node.in_smem:
             idx = self.smem_index(node, args)
             if self.clamp:
@@ -1740,6 +1754,8 @@ class StencilGen(object):
             raise CodegenError("internal: %s read but not available" %
                                f.name)
         else:
+            if self.vec_stats is not None:
+                self.vec_stats[1] += 1      # a strided HBM read
             w("const %s %s = __ldg(b_%s + (%s));" % (
                 ctype(f.typ), t, pg.fn(f),
                 pg.gindex(f, args, ctx, clamp_all=self.clamp)))
@@ -1883,6 +1899,113 @@ class StencilGen(object):
         w("const int %s0 = rr;" % prefix)
 
     # ---- materialized stages -------------------------------------------------
+    # ---- 4-wide interior loops ----------------------------------------------
+    def inner_residues(self):
+        """Per node, the residue mod 4 of the origin of its shared-memory
+        rows (innermost dim) on interior tiles, when every tile has the
+        same one (tile grids starting at a constant); None otherwise."""
+        if hasattr(self, '_res4'):
+            return self._res4
+        from .tiling import infer_regions, _grid_lo
+        plan = self.plan
+        res = {}
+        self._res4 = res
+        self._loop_res = {}
+        glo = _grid_lo(plan)
+        na = plan.anchor.ndims
+        if glo[na - 1] is None:
+            return res
+        env = self.pg.p.int_env()
+        big = 1 << 20
+        samples = []
+        for j in range(3):
+            box = []
+            for k, t in enumerate(plan.tile):
+                lo = (glo[k] if glo[k] is not None else 0) + (big + j) * t
+                box.append((np.asarray([lo]), np.asarray([lo + t - 1])))
+            try:
+                samples.append(infer_regions(plan, box, env, clamp=False))
+            except Exception:
+                return res
+        for n in plan.nodes:
+            if n.role in ('global', 'inline'):
+                continue
+            vals = set(int(np.asarray(reg[n.func][0][-1]).ravel()[0]) % 4
+                       for reg in samples)
+            if len(vals) == 1:
+                self._loop_res[n.func] = vals.pop()
+            if not n.in_smem:
+                continue
+            if n.role == 'stage':
+                lo = _const_int(n.func.domain[-1].lowerBound)
+                if lo is not None:
+                    res[n.func] = lo % 4      # origin d_lo + so, so % 4 == 0
+            elif n.func in self._loop_res:
+                res[n.func] = self._loop_res[n.func]
+        return res
+
+    def choose_vec(self, f, n, ext):
+        """4 points per thread along the innermost dim when every read of
+        the stage from shared memory can then be a 16-byte vector load and
+        none is a strided HBM read (decided by generating the loop once
+        into a scratch buffer)."""
+        pg = self.pg
+        if 'no_vec' in pg.p.options or ext[-1] % 4 or ext[-1] < 16:
+            return 1
+        self.inner_residues()
+        if f not in self._loop_res:
+            return 1
+        saved = pg.w
+        pg.w = self.ctx.w = W()
+        self.ctx.push()
+        self.vec = 4
+        self.vec_stats = [0, 0]
+        try:
+            self.gen_fast_loop(f, n, ext)
+            ok = self.vec_stats[0] > 0 and self.vec_stats[1] == 0
+        finally:
+            self.ctx.pop()
+            pg.w = self.ctx.w = saved
+            self.vec = 1
+            self.vec_stats = None
+        return 4 if ok else 1
+
+    def vec_read(self, node, f, args):
+        """Text of a 16-byte-vector read covering point ``args`` of smem
+        node ``node`` (one lane of a cached float4/int4), or None."""
+        ctx = self.ctx
+        if node.func.typ.size() != 4 or not node.in_smem:
+            return None
+        res = self.inner_residues()
+        if node.func not in res or node._sm_ext[-1] % 4:
+            return None
+        a = args[-1]
+        if is_data_dependent(a):
+            return None
+        fa = affine_form(a)
+        if fa is None:
+            return None
+        coeffs, d = fa
+        if len(coeffs) != 1:
+            return None
+        (v, c), = coeffs.items()
+        if c != 1 or getattr(v, '_cname', None) != self.vec_var:
+            return None
+        vt = {'float': 'float4', 'int': 'int4'}.get(ctype(node.func.typ))
+        if vt is None:
+            return None
+        rc = (self.vec_res + d - res[node.func]) % 4
+        aligned = list(args[:-1]) + [a - rc if rc else a]
+        idx = self.smem_index(node, aligned)
+        key = ('v4', self.node_name(node), idx)
+        t = ctx.lookup(key)
+        if t is None:
+            t = ctx.temp()
+            self.pg.w("const %s %s = *reinterpret_cast<const %s*>(&sm_%s[%s]);"
+                      % (vt, t, vt, self.node_name(node), idx))
+            ctx.define(key, t)
+        return "%s.%s" % (t, "xyzw"[rc])
+
     def gen_step(self, f):
         pg = self.pg
         plan = self.plan
@@ -1898,7 +2021,9 @@ class StencilGen(object):
             if self.has_inside:
                 w.open("if (pm_inside)")
                 self.fast = self.inside = True
+                self.vec = self.choose_vec(f, n, ext)
                 self.gen_fast_loop(f, n, ext)
+                self.vec = 1
                 self.fast = self.inside = False
                 w.close()
                 w.open("else")
@@ -1913,7 +2038,8 @@ class StencilGen(object):
         if n.in_smem:
             w("__syncthreads();")
 
-    def _store(self, f, n, qs, val, flag, smem_idx, gidx=None):
+    def _store(self, f, n, qs, val, flag, smem_idx, gidx=None,
+               hbm=True):
         """Store one computed point: shared memory and/or HBM (owned
         points; pipeline outputs only where some case held)."""
         pg = self.pg
@@ -1922,9 +2048,9 @@ class StencilGen(object):
         nm = self.node_name(n)
         fnm = pg.fn(f)
         nd = n.ndims
-        if n.in_smem:
+        if n.in_smem and smem_idx is not None:
             w("sm_%s[%s] = %s;" % (nm, smem_idx, val))
-        if n.role == 'out':
+        if n.role == 'out' and hbm:
             own = ""
             if n.func is not plan.anchor and n.also_smem:
                 own = " && ".join("%s >= o_%s_lo%d && %s <= o_%s_hi%d" % (
@@ -1970,7 +2096,11 @@ class StencilGen(object):
             w("bool wr = false;")
             flag = "wr"
         self.emit_cases(f, bind, "v", flag)
-        self._store(f, n, ["q%d" % d for d in range(nd)], "v", flag, "i")
+        sidx = "i"
+        if n.in_smem:
+            sidx = " + ".join("j%d * %d" % (d, st) for d, st in
+                              enumerate(n._sm_strides))
+        self._store(f, n, ["q%d" % d for d in range(nd)], "v", flag, sidx)
         ctx.pop()
         w.close()
 
@@ -2008,9 +2138,17 @@ class StencilGen(object):
             cb = ext[0]
             while K > 1 and K * cb > 16:
                 K -= 1
+        V = self.vec if (self.inside and nd >= 2) else 1
+        if V > 1:
+            # 4 consecutive inner points per thread: shared-memory reads of
+            # a row become 16-byte vector loads
+            while K > 1 and K * cb * V > 16:
+                K -= 1
+            self.vec_var = "qb%d" % (nd - 1)
+            self.vec_res = self._loop_res[f]
         nblk = -(-outer // K)
         rest = ext[:-2] if nd >= 2 else []
-        total = nblk * inner
+        total = nblk * (inner // V)
         for d, e in enumerate(rest):
             total *= 1 if (d == 0 and cb > 1) else e
         strides = []
@@ -2020,7 +2158,11 @@ class StencilGen(object):
             st *= e
         w.open("for (int it = threadIdx.x; it < %d; it += %d)" % (
             total, plan.threads))
-        w("const int ji = it %% %d; int rr = it / %d;" % (inner, inner))
+        if V > 1:
+            w("const int ji = (it %% %d) * %d; int rr = it / %d;" % (
+                inner // V, V, inner // V))
+        else:
+            w("const int ji = it %% %d; int rr = it / %d;" % (inner, inner))
         if nd >= 2:
             if outer % K:
                 w("const int jo = pm_imin((rr %% %d) * %d, %d); rr /= %d;" % (
@@ -2043,6 +2185,8 @@ class StencilGen(object):
             else:
                 j = "j%d" % d
             w("const int qb%d = r_%s_lo%d + %s;" % (d, nm, d, j))
+        if n.in_smem:
+            strides = list(n._sm_strides)     # rows may be padded
         w("const int ib = %s;" % " + ".join(
             "(qb%d - r_%s_lo%d) * %d" % (d, nm, d, strides[d])
             for d in range(nd)))
@@ -2060,35 +2204,74 @@ class StencilGen(object):
                 # regions are clamped to the domain: qb >= its lower bound
                 ctx.var_lo["qb%d" % d] = lo
         flagged = n.role == 'out' and comp.is_output
+        # 16-byte stores of the 4 inner points to HBM: the anchor's inner
+        # index is 4-aligned on interior tiles; base and row strides are
+        # checked at run time
+        vst = None
+        if V > 1 and n.role == 'out' and n.func is plan.anchor and \
+                f.typ.size() == 4:
+            dlo = _const_int(f.domain[-1].lowerBound)
+            if dlo is not None and (self._loop_res[f] - dlo) % 4 == 0:
+                vst = {'float': 'float4', 'int': 'int4'}.get(ctype(f.typ))
+                if vst:
+                    w("const bool pm_v4 = ((unsigned long long)b_%s & 15) "
+                      "== 0%s;" % (fnm, "".join(
+                          " && (s_%s_%d & 3) == 0" % (fnm, d)
+                          for d in range(nd - 1))))
+        group = []
         for c in range(cb):
             for k in range(K):
-                pt = list(base)
-                qs = ["qb%d" % d for d in range(nd)]
-                if nd >= 2 and k:
-                    pt[nd - 2] = base[nd - 2] + k
-                    qs[nd - 2] = "(qb%d + %d)" % (nd - 2, k)
-                if c:
-                    pt[0] = base[0] + c
-                    qs[0] = "(qb0 + %d)" % c
-                bind = dict(zip(f.variables, pt))
-                v = "v%d_%d" % (c, k)
-                w("%s %s = 0;" % (ctype(f.typ), v))
-                flag = None
-                if flagged:
-                    flag = "wr%d_%d" % (c, k)
-                    w("bool %s = false;" % flag)
-                self.emit_cases(f, bind, v, flag)
-                off = k * strides[nd - 2] + c * strides[0]
-                idx = "ib" if off == 0 else "ib + %d" % off
-                gidx = None
-                if n.role == 'out':
-                    terms = ["gb"]
-                    if k:
-                        terms.append("%d * s_%s_%d" % (k, fnm, nd - 2))
+                for u in range(V):
+                    pt = list(base)
+                    qs = ["qb%d" % d for d in range(nd)]
+                    if nd >= 2 and k:
+                        pt[nd - 2] = base[nd - 2] + k
+                        qs[nd - 2] = "(qb%d + %d)" % (nd - 2, k)
                     if c:
-                        terms.append("%d * s_%s_0" % (c, fnm))
-                    gidx = " + ".join(terms)
-                self._store(f, n, qs, v, flag, idx, gidx)
+                        pt[0] = base[0] + c
+                        qs[0] = "(qb0 + %d)" % c
+                    if u:
+                        pt[nd - 1] = base[nd - 1] + u
+                        qs[nd - 1] = "(qb%d + %d)" % (nd - 1, u)
+                    bind = dict(zip(f.variables, pt))
+                    v = "v%d_%d_%d" % (c, k, u)
+                    w("%s %s = 0;" % (ctype(f.typ), v))
+                    flag = None
+                    if flagged:
+                        flag = "wr%d_%d_%d" % (c, k, u)
+                        w("bool %s = false;" % flag)
+                    self.emit_cases(f, bind, v, flag)
+                    off = k * strides[nd - 2] + c * strides[0] + u
+                    idx = "ib" if off == 0 else "ib + %d" % off
+                    gidx = None
+                    if n.role == 'out':
+                        terms = ["gb"]
+                        if k:
+                            terms.append("%d * s_%s_%d" % (k, fnm, nd - 2))
+                        if c:
+                            terms.append("%d * s_%s_0" % (c, fnm))
+                        if u:
+                            terms.append("%d" % u)
+                        gidx = " + ".join(terms)
+                    self._store(f, n, qs, v, flag, idx, gidx,
+                                hbm=vst is None)
+                    if vst is None:
+                        continue
+                    group.append((qs, v, flag, gidx))
+                    if u < V - 1:
+                        continue
+                    cond = " && ".join(["pm_v4"] + [g[2] for g in group
+                                                    if g[2]])
+                    w.open("if (%s)" % cond)
+                    w("*reinterpret_cast<%s*>(&b_%s[%s]) = make_%s(%s);" % (
+                        vst, fnm, group[0][3], vst,
+                        ", ".join(g[1] for g in group)))
+                    w.close()
+                    w.open("else")
+                    for gq, gv, gf, gi in group:
+                        self._store(f, n, gq, gv, gf, None, gi)
+                    w.close()
+                    group = []
         ctx.var_lo = saved_lo
         ctx.pop()
         w.close()

@@ -835,6 +835,11 @@ def _layout_smem(plan):
             w = ((ext[-1] + al - 1 + al - 1) // al) * al
             n.pad_inner = w
             ext[-1] = w
+        elif es == 4 and ext[-1] % 4 and ext[-1] > 4:
+            # rows of whole 16-byte chunks, so that the interior path can
+            # read four consecutive points with one vector load
+            n.pad_inner = ((ext[-1] + 3) // 4) * 4
+            ext[-1] = n.pad_inner
         nbytes = es
         for e in ext:
             nbytes *= e
