@@ -333,6 +333,8 @@ def run(args):
                 for a in measure.APPS)
             line["pipelines"]["bilateral_batch64"] = \
                 measure.measure_bilateral_batch(64, device=dev)
+            line["pipelines"]["stream1024"] = measure.measure_stream(
+                1024, device=dev)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line))

@@ -179,15 +179,38 @@ def measure_bilateral_batch(n=64, steps=10, warmup=3, graph=True,
             "l2": "256 MB written before each timed run"}
 
 
+def measure_stream(n=1024, seed=1, device=None):
+    """The mixed request stream (``polymage_b200.apps.stream``): ``n``
+    Harris / unsharp / pyramid requests with sides U{256..4096}, served in
+    per-pipeline batches; MPix/s and compulsory-bytes roofline over the
+    batch calls' GPU time."""
+    from . import stream
+    reqs = stream.make_stream(n, seed)
+    r = stream.serve(reqs, device=device, seed=seed)
+    peak, kind = hbm_peak()
+    gbs = r["bytes"] / (r["ms"] / 1e3) / 1e9
+    return {"app": "stream%d" % n,
+            "workload": "%d requests (Harris, unsharp, pyramid L=4), sides "
+                        "U{256..4096} seed %d, %.1f GPix" % (
+                            n, seed, r["pixels"] / 1e9),
+            "ms": r["ms"], "mpix_s": r["pixels"] / (r["ms"] / 1e3) / 1e6,
+            "chunks": r["chunks"], "batch_calls": r["batch_calls"],
+            "compulsory_bytes": int(r["bytes"]), "achieved_gbs": gbs,
+            "hbm_frac": gbs / peak, "peak_gbs": peak, "peak_source": kind,
+            "l2": "inputs of each chunk (8 GB) larger than L2"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--app", action="append",
-                    choices=APPS + ("bilateral_batch64",))
+                    choices=APPS + ("bilateral_batch64", "stream1024"))
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     args = ap.parse_args()
-    for app in args.app or APPS + ("bilateral_batch64",):
-        if app == "bilateral_batch64":
+    for app in args.app or APPS + ("bilateral_batch64", "stream1024"):
+        if app == "stream1024":
+            print(json.dumps(measure_stream(1024)))
+        elif app == "bilateral_batch64":
             print(json.dumps(measure_bilateral_batch(
                 64, steps=min(args.steps, 10), warmup=args.warmup)))
         else:
