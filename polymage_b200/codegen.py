@@ -53,6 +53,7 @@ points of a pipeline output not covered by any ``Case`` are left untouched,
 as in the reference.
 """
 
+import math
 import re
 
 import numpy as np
@@ -165,6 +166,10 @@ class ExprCtx(object):
         # lower bounds of loop variables (C name -> int), for emitting
         # unsigned division/modulo where the numerator cannot be negative
         self.var_lo = {}
+        # residues of loop variables known at compile time
+        # (C name -> (residue, modulus)), for folding x % k and parity
+        # Selects on interior tiles
+        self.var_res = {}
 
     def temp(self):
         self.ntemp += 1
@@ -227,6 +232,10 @@ class ExprCtx(object):
             args = [_subst(a, bind) for a in e.arguments]
             return self.reader(e.objectRef, args, self)
         if isinstance(e, AbstractBinaryOpNode):
+            if e.op == '%':
+                sm = self._static_mod(e, bind)
+                if sm is not None:
+                    return str(sm)
             if e.op in ('/', '%') and self._unsigned_ok(e, bind):
                 # truncating division of a non-negative int by a positive
                 # constant equals unsigned division (a shift or mask for
@@ -240,6 +249,12 @@ class ExprCtx(object):
         if isinstance(e, C.Cast):
             return "((%s)(%s))" % (ctype(e.typ), self.expr(e.expression, bind))
         if isinstance(e, C.Select):
+            sv = self._static_cond(e.condition, bind)
+            if sv is not None:
+                # the condition is known here: only the taken arm is
+                # evaluated (the arms have no side effects)
+                return self.expr(e.true_expression if sv else
+                                 e.false_expression, bind)
             c = self.cond(e.condition, bind)
             a = self.expr(e.true_expression, bind)
             b = self.expr(e.false_expression, bind)
@@ -283,6 +298,57 @@ class ExprCtx(object):
                 return False
             low += c * lo
         return low >= 0
+
+    def _static_mod(self, e, bind):
+        """Value of ``x % k`` when the residues of its loop variables are
+        known and x cannot be negative; else None."""
+        if not self.var_res:
+            return None
+        r = e.right
+        if not (isinstance(r, Value) and r.typ in _INT_T and
+                int(r.value) > 0) or not self._unsigned_ok(e, bind):
+            return None
+        m = int(r.value)
+        f = affine_form(_subst(e.left, bind))
+        if f is None:
+            return None
+        total = f[1]
+        for v, c in f[0].items():
+            rm = self.var_res.get(getattr(v, '_cname', None))
+            if rm is None or rm[1] % m:
+                return None
+            total += c * rm[0]
+        return total % m
+
+    def _static_int(self, e, bind):
+        e = Value.numericToValue(e)
+        if isinstance(e, Value):
+            return int(e.value) if e.typ in _INT_T else None
+        if isinstance(e, AbstractBinaryOpNode) and e.op == '%':
+            return self._static_mod(e, bind)
+        return None
+
+    def _static_cond(self, c, bind):
+        """True/False when condition ``c`` is decided by known residues."""
+        if not self.var_res:
+            return None
+        op = c.conditional
+        if op in ('&&', '||'):
+            a = self._static_cond(c.lhs, bind)
+            b = self._static_cond(c.rhs, bind)
+            if op == '&&':
+                if a is False or b is False:
+                    return False
+                return True if (a and b) else None
+            if a is True or b is True:
+                return True
+            return False if (a is False and b is False) else None
+        a = self._static_int(c.lhs, bind)
+        b = self._static_int(c.rhs, bind)
+        if a is None or b is None:
+            return None
+        return {'==': a == b, '!=': a != b, '<': a < b, '<=': a <= b,
+                '>': a > b, '>=': a >= b}.get(op)
 
     def cond(self, c, bind):
         op = c.conditional
@@ -1911,29 +1977,39 @@ class StencilGen(object):
         res = {}
         self._res4 = res
         self._loop_res = {}
+        self._lo_res = {}
         glo = _grid_lo(plan)
         na = plan.anchor.ndims
         if glo[na - 1] is None:
             return res
         env = self.pg.p.int_env()
         big = 1 << 20
-        samples = []
-        for j in range(3):
-            box = []
-            for k, t in enumerate(plan.tile):
-                lo = (glo[k] if glo[k] is not None else 0) + (big + j) * t
-                box.append((np.asarray([lo]), np.asarray([lo + t - 1])))
-            try:
-                samples.append(infer_regions(plan, box, env, clamp=False))
-            except Exception:
-                return res
+        # far interior tiles, 8 consecutive along every anchor dim (a full
+        # period of any residue mod 8 of a region origin whose scale
+        # factors divide the tile sizes; others show up as several values)
+        grids = np.meshgrid(*[np.arange(8, dtype=np.int64)] * na,
+                            indexing='ij')
+        box = []
+        for k, t in enumerate(plan.tile):
+            lo = (glo[k] if glo[k] is not None else 0) + \
+                (big + grids[k].ravel()) * t
+            box.append((lo, lo + t - 1))
+        try:
+            reg = infer_regions(plan, box, env, clamp=False)
+        except Exception:
+            return res
+
+        def residues(n, d, m):
+            v = np.unique(np.asarray(reg[n.func][0][d]).ravel() % m)
+            return int(v[0]) if len(v) == 1 else None
         for n in plan.nodes:
             if n.role in ('global', 'inline'):
                 continue
-            vals = set(int(np.asarray(reg[n.func][0][-1]).ravel()[0]) % 4
-                       for reg in samples)
-            if len(vals) == 1:
-                self._loop_res[n.func] = vals.pop()
+            r4 = residues(n, n.ndims - 1, 4)
+            if r4 is not None:
+                self._loop_res[n.func] = r4
+            self._lo_res[n.func] = [residues(n, d, 8)
+                                    for d in range(n.ndims)]
             if not n.in_smem:
                 continue
             if n.role == 'stage':
@@ -2198,11 +2274,28 @@ class StencilGen(object):
         ctx = self.ctx
         ctx.push()
         saved_lo = dict(ctx.var_lo)
+        saved_res = dict(ctx.var_res)
         for d, dom in enumerate(f.domain):
             lo = _const_int(dom.lowerBound)
             if lo is not None:
                 # regions are clamped to the domain: qb >= its lower bound
                 ctx.var_lo["qb%d" % d] = lo
+        if self.inside and 'no_static_res' not in pg.p.options:
+            # interior tiles: region origins have fixed residues (mod 8),
+            # and block starts are multiples of the block sizes
+            self.inner_residues()
+            lres = self._lo_res.get(f) or [None] * nd
+            for d in range(nd):
+                if lres[d] is None:
+                    continue
+                if d == nd - 1:
+                    m = math.gcd(V, 8) if V > 1 else 1
+                elif d == nd - 2 and outer % K == 0:
+                    m = math.gcd(K, 8)
+                else:
+                    m = 1
+                if m > 1:
+                    ctx.var_res["qb%d" % d] = (lres[d] % m, m)
         flagged = n.role == 'out' and comp.is_output
         # 16-byte stores of the 4 inner points to HBM: the anchor's inner
         # index is 4-aligned on interior tiles; base and row strides are
@@ -2273,6 +2366,7 @@ class StencilGen(object):
                     w.close()
                     group = []
         ctx.var_lo = saved_lo
+        ctx.var_res = saved_res
         ctx.pop()
         w.close()
 

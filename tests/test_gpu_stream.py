@@ -25,7 +25,9 @@ def test_mixed_stream_matches_oracle(cuda):
             img = ins['img'].cpu().numpy()
             ref = OH.harris(img)
             got = outs['harris'].cpu().numpy()
-            inner = (slice(2, img.shape[0] - 1), slice(2, img.shape[1] - 1))
+            # written: [2, rows-3] x [2, cols-3] (the outputs start
+            # uninitialized, so only written points are compared)
+            inner = (slice(2, img.shape[0] - 2), slice(2, img.shape[1] - 2))
             err = np.abs(got[inner] - ref[inner]).max() / np.abs(ref).max()
             assert err <= 1e-5, err
         elif kind == 'unsharp':
