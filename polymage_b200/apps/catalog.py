@@ -4,7 +4,11 @@ the best of exhaustive tuning on B200 at each pipeline's benchmark size
 timed runs each with L2 flushed; polymage_b200.autotune).  Harris keeps the
 group size of the reference's Harris builder (11: all stages in one group,
 harris/builder.py:66-67), which is outside the tuned group sizes (3..10)
-and faster than their best (0.029 vs 0.034 ms)."""
+and faster than their best (0.029 vs 0.034 ms).  Unsharp recomputes blurx
+inside blury (a larger inline budget) on 128x128 tiles, also outside the
+tuned space: with 16-byte shared-memory reads the recomputation is cheaper
+than a second shared-memory stage and its barrier (0.087-0.090 vs
+0.094 ms for the tuned best)."""
 
 import functools
 
@@ -15,7 +19,8 @@ from .bilateral_grid import build_bilateral
 from .pyramid_blend import build_pyramid
 
 HARRIS = dict(tile_sizes=(16, 128), group_size=11, options=('rblock=8',))
-UNSHARP = dict(tile_sizes=(64, 128), group_size=10, options=('rblock=8',))
+UNSHARP = dict(tile_sizes=(128, 128), group_size=10,
+               options=('rblock=8', 'inline_budget=400'))
 CAMPIPE = dict(tile_sizes=(32, 64), group_size=9, options=('rblock=8',))
 BILATERAL = dict(tile_sizes=(1, 32, 128), group_size=10,
                  options=(('red_tile', (32, 256)), 'rblock=4'))
