@@ -122,3 +122,71 @@ def make_inputs(R, C, seed=0):
     img2 = rng.random((3, R, C), dtype=np.float32)
     mask = rng.random((R, C), dtype=np.float32)
     return img1, img2, mask
+
+
+# ---------------------------------------------------------------------------
+# Generalized spec: any number of levels on any image size, indices clamped
+# to each level's domain (polymage_b200/apps/pyramid_blend.py,
+# pyramid_blending_clamped).  The filters are the reference's
+# (polymage_blending.py:42-194); only the boundary handling differs.
+
+def _down_rows(g):
+    """5-tap [1,4,6,4,1]/16 decimation by 2 along axis -2, clamped."""
+    n = g.shape[-2]
+    m = (n + 1) // 2
+    x = np.arange(m)
+    w = (1, 4, 6, 4, 1)
+    out = 0.0
+    for k in range(5):
+        idx = np.clip(2 * x + k - 2, 0, n - 1)
+        out = out + w[k] * np.take(g, idx, axis=-2)
+    return out * 0.0625
+
+
+def _down(g):
+    return np.swapaxes(_down_rows(np.swapaxes(_down_rows(g), -1, -2)),
+                       -1, -2)
+
+
+def _up_rows(g, n):
+    """Level-l+1 rows interpolated to ``n`` rows (even: [1,6,1]/8, odd:
+    [4,4]/8), clamped."""
+    m = g.shape[-2]
+    x = np.arange(n)
+    h = x // 2
+    lo = np.clip(h - 1, 0, m - 1)
+    hi = np.clip(h + 1, 0, m - 1)
+    gh = np.take(g, h, axis=-2)
+    even = (np.take(g, lo, axis=-2) + 6 * gh + np.take(g, hi, axis=-2)) * \
+        0.125
+    odd = (4 * gh + 4 * np.take(g, hi, axis=-2)) * 0.125
+    sel = (x % 2 == 0).reshape((-1, 1))
+    return np.where(sel, even, odd)
+
+
+def _up(g, n_rows, n_cols):
+    u = _up_rows(g, n_rows)
+    return np.swapaxes(_up_rows(np.swapaxes(u, -1, -2), n_cols), -1, -2)
+
+
+def pyramid_blend_clamped(img1, img2, mask, L=8):
+    """img1, img2: [3][R][C]; mask: [R][C] -> float64 [3][R][C]."""
+    g1 = [np.asarray(img1, np.float64)]
+    g2 = [np.asarray(img2, np.float64)]
+    gm = [np.asarray(mask, np.float64)]
+    for _ in range(1, L):
+        g1.append(_down(g1[-1]))
+        g2.append(_down(g2[-1]))
+        gm.append(_down(gm[-1]))
+
+    def lap(g, l):
+        if l == L - 1:
+            return g[l]
+        r, c = g[l].shape[-2:]
+        return g[l] - _up(g[l + 1], r, c)
+    res = [lap(g1, l) * gm[l] + lap(g2, l) * (1 - gm[l]) for l in range(L)]
+    out = res[L - 1]
+    for l in range(L - 2, -1, -1):
+        r, c = res[l].shape[-2:]
+        out = res[l] + _up(out, r, c)
+    return out

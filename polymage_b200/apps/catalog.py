@@ -17,7 +17,7 @@ from .harris import build_harris
 from .unsharp_mask import build_unsharp
 from .campipe import build_campipe
 from .bilateral_grid import build_bilateral
-from .pyramid_blend import build_pyramid
+from .pyramid_blend import build_pyramid, build_pyramid_clamped
 
 HARRIS = dict(tile_sizes=(16, 128), group_size=11, options=('rblock=8',))
 UNSHARP = dict(tile_sizes=(128, 128), group_size=10,
@@ -26,6 +26,9 @@ CAMPIPE = dict(tile_sizes=(32, 64), group_size=12, options=('rblock=8',))
 BILATERAL = dict(tile_sizes=(1, 32, 128), group_size=10,
                  options=(('red_tile', (32, 256)), 'rblock=4'))
 PYRAMID = dict(tile_sizes=(32, 64), group_size=10, options=('rblock=8',))
+# 8 levels, indices clamped at every level's borders (any image size)
+PYRAMID8 = dict(L=8, tile_sizes=(32, 64), group_size=10,
+                options=('rblock=8',))
 
 _BUILDERS = {
     "harris": (build_harris, HARRIS),
@@ -33,6 +36,7 @@ _BUILDERS = {
     "campipe": (build_campipe, CAMPIPE),
     "bilateral": (build_bilateral, BILATERAL),
     "pyramid": (build_pyramid, PYRAMID),
+    "pyramid8": (build_pyramid_clamped, PYRAMID8),
 }
 
 _cache = {}

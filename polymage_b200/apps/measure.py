@@ -21,7 +21,7 @@ import numpy as np
 
 from . import catalog
 
-APPS = ("harris", "unsharp", "campipe", "bilateral", "pyramid")
+APPS = ("harris", "unsharp", "campipe", "bilateral", "pyramid", "pyramid8")
 FLUSH_BYTES = 256 << 20
 
 
@@ -67,6 +67,14 @@ def workload(app, seed=0):
                 {'blend': ((3, R - 60, C - 60), np.float32)},
                 (R - 60) * (C - 60),
                 "pyramid_blend L=4 3x2108x2108 float32")
+    if app == 'pyramid8':
+        R = C = 2048
+        return ({'R': R, 'C': C},
+                {'img1': rng.random((3, R, C), dtype=np.float32),
+                 'img2': rng.random((3, R, C), dtype=np.float32),
+                 'mask': rng.random((R, C), dtype=np.float32)},
+                {'blend': ((3, R, C), np.float32)}, R * C,
+                "pyramid_blend L=8 (clamped borders) 3x2048x2048 float32")
     raise ValueError(app)
 
 
@@ -193,7 +201,7 @@ def measure_stream(n=1024, seed=1, device=None):
     peak, kind = hbm_peak()
     gbs = r["bytes"] / (r["ms"] / 1e3) / 1e9
     return {"app": "stream%d" % n,
-            "workload": "%d requests (Harris, unsharp, pyramid L=4), sides "
+            "workload": "%d requests (Harris, unsharp, pyramid L=8), sides "
                         "U{256..4096} seed %d, %.1f GPix" % (
                             n, seed, r["pixels"] / 1e9),
             "ms": r["ms"], "mpix_s": r["pixels"] / (r["ms"] / 1e3) / 1e6,

@@ -11,10 +11,11 @@ CTAs the GPU holds at once).  Request inputs are created on the device
 (U[0,1)); the timed region of a chunk is its batch calls only, bracketed by
 CUDA events on the launching stream.
 
-Pyramid requests use the reference's 4-level spec
-(pyramid_blend/polymage_blending.py:24): at 8 levels its boundary margins
-(2^(L+1) pixels) leave references outside the domains for every size in
-the stream.
+Pyramid requests blend with 8 levels and indices clamped at each level's
+borders (``pyramid_blending_clamped``): the reference's spec
+(pyramid_blend/polymage_blending.py:24, 4 levels) shrinks its domains by
+2^(L+1) pixels per side, which at 8 levels leaves references outside the
+domains for every size in the stream.
 """
 
 import argparse
@@ -24,7 +25,7 @@ import numpy as np
 
 from . import catalog
 
-KINDS = ("harris", "unsharp", "pyramid")
+KINDS = ("harris", "unsharp", "pyramid8")
 
 
 def make_stream(n=1024, seed=1, lo=256, hi=4096):
@@ -43,7 +44,7 @@ def request_bytes(kind, r, c):
         return 8 * r * c, r * c
     if kind == 'unsharp':
         return 4 * 3 * ((r + 4) * (c + 4) + r * c), r * c
-    return 4 * (7 * r * c + 3 * (r - 60) * (c - 60)), (r - 60) * (c - 60)
+    return 4 * (7 * r * c + 3 * r * c), r * c
 
 
 def _request_io(kind, r, c, dev, gen):
@@ -60,7 +61,7 @@ def _request_io(kind, r, c, dev, gen):
                 {'mask': torch.empty((3, r, c), device=dev)})
     return ({'R': r, 'C': c},
             {'img1': rnd(3, r, c), 'img2': rnd(3, r, c), 'mask': rnd(r, c)},
-            {'blend': torch.empty((3, r - 60, c - 60), device=dev)})
+            {'blend': torch.empty((3, r, c), device=dev)})
 
 
 def serve(reqs, device=None, budget=8 << 30, seed=1, keep=False):

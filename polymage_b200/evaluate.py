@@ -118,8 +118,18 @@ def try_eval_int(expr, env):
         return None
 
 
+def _has_loop_var(e):
+    return any(not isinstance(v, C.Parameter)
+               for v in e.collect(C.Variable)) if hasattr(e, 'collect') \
+        else False
+
+
 def divisors_in(expr):
-    """Positive integer divisors used by ``/`` nodes in an expression."""
+    """Positive integer divisors used by ``/`` nodes whose numerator
+    varies with a (non-parameter) variable: the divisions that make an
+    index periodic in that variable.  Divisions of parameters and literals
+    only (a level size ``(R + 63) / 64`` in a clamp bound) are constants
+    and contribute nothing."""
     out = []
     stack = [expr]
     while stack:
@@ -127,11 +137,23 @@ def divisors_in(expr):
         if isinstance(n, AbstractBinaryOpNode) and n.op == '/':
             r = n.right
             if isinstance(r, Value) and isinstance(r.value, int) and \
-                    r.value > 0:
+                    r.value > 0 and _has_loop_var(n.left):
                 out.append(r.value)
         if hasattr(n, 'children'):
             stack.extend(n.children())
     return out
+
+
+def is_min_max(e):
+    """Whether a Select is a max or min of its two arms (``a > b ? a : b``
+    and the like, also after cloning, which loses the Max/Min classes)."""
+    if not isinstance(e, C.Select):
+        return False
+    c = e.condition
+    if c.conditional not in ('<', '<=', '>', '>='):
+        return False
+    t, f = str(e.true_expression), str(e.false_expression)
+    return (str(c.lhs), str(c.rhs)) in ((t, f), (f, t))
 
 
 def monotone_dir(expr, var):
@@ -188,5 +210,17 @@ def monotone_dir(expr, var):
                     not isinstance(r.value, int) or r.value == 0:
                 return None
             return a if r.value > 0 else -a
+        return None
+    if is_min_max(expr):
+        # the max/min of two functions monotone in the same direction (or
+        # constant in var) is monotone in that direction: clamped indices
+        a = monotone_dir(expr.true_expression, var)
+        b = monotone_dir(expr.false_expression, var)
+        if a is None or b is None:
+            return None
+        if a == 0:
+            return b
+        if b == 0 or a == b:
+            return a
         return None
     return None

@@ -51,7 +51,7 @@ import numpy as np
 from . import constructs as C
 from .expr_ast import Value, AbstractBinaryOpNode, InbuiltFunction
 from .expression import substitute_vars
-from .evaluate import (eval_int, EvalError, monotone_dir, divisors_in,
+from .evaluate import (is_min_max, eval_int, EvalError, monotone_dir, divisors_in,
                        try_eval_int)
 
 SMEM_BUDGET = 200 * 1024       # bytes per CTA we allow a plan to use
@@ -108,9 +108,15 @@ class IndexFn(object):
 
 
 def is_data_dependent(e):
+    """Whether an index expression depends on data (or is not integer
+    arithmetic that region inference can follow).  Max/Min of index
+    arithmetic (clamped indices) are not data dependent."""
     stack = [e]
     while stack:
         n = stack.pop()
+        if is_min_max(n):
+            stack.extend([n.true_expression, n.false_expression])
+            continue
         if isinstance(n, (C.Reference, C.Select, C.Cast, InbuiltFunction)):
             return True
         if isinstance(n, AbstractBinaryOpNode) and n.op not in ('+', '-',
@@ -615,6 +621,11 @@ def infer_regions(plan, anchor_box, env, clamp=True, tile_first=None):
     be arrays).  ``anchor_box``: [(lo, hi)] per anchor dim.  ``tile_first``:
     per anchor dim, whether the tile is the first along that dim (used for
     ownership of lower-dimensional live-outs)."""
+    if not clamp:
+        # unclamped regions model interior tiles far from every border:
+        # parameters are taken huge so that indices clamped to a
+        # parameter-dependent bound (min/max) behave as in the interior
+        env = dict((k, 1 << 40) for k in env)
     regions = {}
     big = 1 << 60
     for n in plan.nodes:
@@ -787,6 +798,8 @@ def _alignment(plan, env):
     composed monotone index functions (slope measured over a long span)."""
     K = 1 << 16
     base = 1 << 20
+    # interior behaviour: parameter-dependent clamps must not bind
+    env = dict((k, 1 << 40) for k in env)
     for n in plan.nodes:
         n.align = [None] * n.ndims
         n.scale = [None] * n.ndims

@@ -1,8 +1,9 @@
-"""A small mixed request stream (Harris, unsharp mask, pyramid blending on
-uneven sizes) served in batches under a tight memory budget, so that it is
-cut into several chunks; every request's output is checked against the
-oracle with the single-image tolerances (Harris 1e-5 relative, unsharp
-1e-5 where the select margin exceeds 1e-6, pyramid 2e-5)."""
+"""A small mixed request stream (Harris, unsharp mask, 8-level pyramid
+blending on uneven sizes) served in batches under a tight memory budget,
+so that it is cut into several chunks; every request's output is checked
+against the oracle with the single-image tolerances (Harris 1e-5
+relative, unsharp 1e-5 where the select margin exceeds 1e-6, pyramid
+2e-5)."""
 
 import numpy as np
 import pytest
@@ -40,9 +41,9 @@ def test_mixed_stream_matches_oracle(cuda):
             d = np.abs(outs['mask'].cpu().numpy().astype(np.float64) - ref)
             assert d[ok].max() <= 1e-5, d[ok].max()
         else:
-            ref = OP.pyramid_blend(ins['img1'].cpu().numpy(),
-                                   ins['img2'].cpu().numpy(),
-                                   ins['mask'].cpu().numpy())
+            ref = OP.pyramid_blend_clamped(ins['img1'].cpu().numpy(),
+                                           ins['img2'].cpu().numpy(),
+                                           ins['mask'].cpu().numpy(), L=8)
             err = np.abs(outs['blend'].cpu().numpy().astype(np.float64) -
                          ref).max()
             assert err <= 2e-5, err

@@ -44,3 +44,17 @@ def test_unsharp_convention_outside_defined_region():
     out = OU.unsharp(img, 0.001, 3.0)
     assert out.shape == (3, 10, 12)
     assert np.all(out[:, 9, :] == 0) and np.all(out[:, :, 11] == 0)
+
+
+def test_clamped_pyramid_oracle_matches_reference_spec_inside():
+    """The generalized (clamped) pyramid spec at L = 4 equals the
+    reference's 4-level spec on the reference's output box, where no
+    clamp is reached."""
+    import oracle.pyramid as OP
+    R, C = 157, 211
+    img1, img2, mask = OP.make_inputs(R, C, seed=2)
+    ref = OP.pyramid_blend(img1, img2, mask, L=4)
+    gen = OP.pyramid_blend_clamped(img1, img2, mask, L=4)
+    (x0, x1), (y0, y1) = OP.output_box(R, C)
+    assert ref.shape == (3, x1 - x0 + 1, y1 - y0 + 1)
+    assert np.abs(gen[:, x0:x1 + 1, y0:y1 + 1] - ref).max() < 1e-12
