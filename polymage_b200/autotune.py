@@ -24,7 +24,7 @@ from .apps.harris import harris_pipe
 from .apps.unsharp_mask import unsharp_mask
 from .apps.campipe import camera_pipe, MATRIX_3200, MATRIX_7000
 from .apps.bilateral_grid import bilateral_grid
-from .apps.pyramid_blend import pyramid_blending
+from .apps.pyramid_blend import pyramid_blending, pyramid_blending_clamped
 from .constructs import Condition
 
 
@@ -73,6 +73,15 @@ def app_setup(app, seed=0):
                 'img2': rng.random((3, R, C), dtype=np.float32),
                 'mask': rng.random((R, C), dtype=np.float32),
                 'blend': np.zeros((3, R - 60, C - 60), np.float32)}
+    elif app == 'pyramid8':
+        out = pyramid_blending_clamped(d, L=8)
+        R = C = 2048
+        est = [(d['R'], R), (d['C'], C)]
+        data = {'R': R, 'C': C,
+                'img1': rng.random((3, R, C), dtype=np.float32),
+                'img2': rng.random((3, R, C), dtype=np.float32),
+                'mask': rng.random((R, C), dtype=np.float32),
+                'blend': np.zeros((3, R, C), np.float32)}
     else:
         raise ValueError(app)
     arg = {'_tuner_app_name': app, '_tuner_live_outs': [out],

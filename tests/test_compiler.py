@@ -97,3 +97,49 @@ def test_grouping_respects_group_size():
     p = build_harris(tile_sizes=(32, 128), group_size=3)
     assert all(len(g.comps) <= 3 for g in p.groups)
     assert len(p.groups) > 1
+
+
+def test_clamped_taps_are_monotone():
+    """min/max of indices monotone in the same direction are monotone (the
+    clamped taps of the 8-level pyramid)."""
+    from polymage_b200.evaluate import is_min_max, monotone_dir
+    R = Parameter(Int, "R")
+    x = Variable(Int, "x")
+    e = Min(Max(2 * x - 2, 0), (R + 63) / 64 - 1)
+    assert is_min_max(e)
+    assert monotone_dir(e, x) == 1
+    assert monotone_dir(Min(Max(7 - x, 0), R - 1), x) == -1
+    assert monotone_dir(Max(x, 5 - x), x) is None
+
+
+def test_level_size_divisions_do_not_enter_the_period():
+    """A stage decimating a level whose size is (R + 63) / 64: the tile
+    origin period is 1 (the division is of parameters only), and the
+    staged producer's static extent covers the clamped 5-tap footprint of
+    a 32-row tile (2 * 32 + 3 rows)."""
+    from polymage_b200.evaluate import divisors_in
+    R = Parameter(Int, "R")
+    C = Parameter(Int, "C")
+    x = Variable(Int, "x")
+    y = Variable(Int, "y")
+    n6 = (R + 63) / 64
+    n7 = (R + 127) / 128
+    img = Image(Float, "img", [R, C])
+    a = Function(([x, y], [Interval(Int, 0, n6 - 1), Interval(Int, 0, C - 1)]),
+                 Float, "a")
+    a.defn = [img(Min(64 * x, R - 1), y) * 0.5]
+    b = Function(([x, y], [Interval(Int, 0, n7 - 1), Interval(Int, 0, C - 1)]),
+                 Float, "b")
+    w = (1, 4, 6, 4, 1)
+    b.defn = [sum(w[k] * a(Min(Max(2 * x + k - 2, 0), n6 - 1), y)
+                  for k in range(5)) * 0.0625]
+    assert divisors_in(Min(Max(2 * x - 2, 0), n6 - 1)) == []
+    assert divisors_in(x / 2 + n6) == [2]
+    p = buildPipeline([b], param_estimates=[(R, 2048), (C, 2048)],
+                      tile_sizes=[32, 64], group_size=2,
+                      options=[('materialize', ['a'])])
+    assert len(p.groups) == 1
+    plan = p.groups[0].plan
+    assert plan.period == 1
+    ext = dict((n.name, n.ext) for n in plan.nodes)
+    assert ext['a'] == [67, 64]
