@@ -71,6 +71,11 @@ _INT_T = (C.Int, C.UInt, C.Short, C.UShort, C.Char, C.UChar, C.Long,
           C.ULong)
 
 
+# concurrent streams of the single-image entry points (option 'streams=N';
+# 1 launches every group on the caller's stream)
+DEFAULT_STREAMS = 4
+
+
 class CodegenError(Exception):
     pass
 
@@ -647,6 +652,99 @@ class PipelineGen(object):
             return "ctab_ptr_%s" % self.fn(f)
         raise CodegenError("no buffer for %s" % f.name)
 
+    def buf_key(self, f):
+        """Identity of the HBM buffer holding ``f`` (None for stages kept
+        in shared memory or registers)."""
+        if any(f is x for x in self.inputs):
+            return ('in', id(f))
+        if any(f is x for x in self.outputs):
+            return ('out', id(f))
+        comp = self.p.func_map.get(f)
+        if comp is not None and comp in self.slot_of:
+            return ('slot', self.slot_of[comp])
+        if getattr(f, 'is_const_func', False):
+            return ('ctab', id(f))
+        return None
+
+    def group_rw(self, g):
+        """(buffers read, buffers written) by one group's launch."""
+        from .pipe import body_refs
+        funcs = [c.func for c in g.comps]
+        ids = set(id(f) for f in funcs)
+        reads, writes = set(), set()
+        for f in funcs:
+            k = self.buf_key(f)
+            if k is not None:
+                writes.add(k)
+            for r in body_refs(f):
+                x = r.objectRef
+                if id(x) in ids:
+                    continue
+                k = self.buf_key(x)
+                if k is not None:
+                    reads.add(k)
+        return reads, writes
+
+    def schedule(self):
+        """(stream of each launch, waits, recorded launches) of the
+        concurrent schedule (polymage_b200.streams)."""
+        if getattr(self, '_sched', None) is None:
+            from . import streams
+            nst = int(_opt(self.p, 'streams', DEFAULT_STREAMS))
+            self._sched = streams.schedule(self.launch_rw, nst,
+                                           main_only=self.launch_main)
+        return self._sched
+
+    def emit_calls(self, w, calls, ret):
+        """Every group's launch in program order, spread over concurrent
+        streams when groups are independent.  ``calls[j]``: the C call of
+        launch j with ``{s}`` where its stream goes (it returns a status);
+        ``ret``: the statement that returns a failed ``st``.  The caller's
+        stream ``s`` forks to the side streams first and joins them at the
+        end, also when a launch fails."""
+        sof, waits, records = self.schedule()
+        used = sorted(set(sof) - {0})
+        if not used:
+            for c in calls:
+                w("if ((st = %s)) %s" % (c.format(s="s"), ret))
+            return
+        ev = {}
+        for i in sorted(records):
+            ev[i] = len(ev) + 1
+        join = dict((k, len(ev) + 1 + n) for n, k in enumerate(used))
+        nev = 1 + len(ev) + len(used)
+        self.conc_streams = max(self.conc_streams, max(used))
+        self.conc_events = max(self.conc_events, nev)
+        w("// %d launches on %d streams: independent groups run "
+          "concurrently" % (len(sof), len(used) + 1))
+        w.open("")
+        w("cudaStream_t ss[%d]; ss[0] = s;" % (max(used) + 1))
+        w("cudaEvent_t* ev = nullptr;")
+        w("if ((st = pm_conc_get(ss, %d, %d, &ev))) %s" % (max(used), nev,
+                                                          ret))
+        w("if (cudaEventRecord(ev[0], s) != cudaSuccess) { st = "
+          "PM_ERR_CUDA; %s }" % ret)
+        for k in used:
+            w("if (cudaStreamWaitEvent(ss[%d], ev[0], 0) != cudaSuccess) { st "
+              "= PM_ERR_CUDA; %s }" % (k, ret))
+        w.open("do")
+        for j, c in enumerate(calls):
+            for i in waits[j]:
+                w("if (cudaStreamWaitEvent(ss[%d], ev[%d], 0) != cudaSuccess)"
+                  " { st = PM_ERR_CUDA; break; }" % (sof[j], ev[i]))
+            w("if ((st = %s)) break;" % c.format(s="ss[%d]" % sof[j]))
+            if j in records:
+                w("if (cudaEventRecord(ev[%d], ss[%d]) != cudaSuccess) "
+                  "{ st = PM_ERR_CUDA; break; }" % (ev[j], sof[j]))
+        w.close("} while (0);")
+        w("// join: the caller's stream follows every side stream")
+        for k in used:
+            w("if (cudaEventRecord(ev[%d], ss[%d]) != cudaSuccess || "
+              "cudaStreamWaitEvent(s, ev[%d], 0) != cudaSuccess) st = st ? "
+              "st : PM_ERR_CUDA;" % (join[k], k, join[k]))
+        w("if (st) %s" % ret)
+        w.close()
+
     # ---- entry points -----------------------------------------------------------
     def abi_params(self):
         ps = ["%s %s" % (self.ptype(q), q.name) for q in self.params]
@@ -657,8 +755,6 @@ class PipelineGen(object):
     def gen_entries(self):
         w = self.w
         name = self.pname
-        launches = self.launch_fns
-        ctx = ExprCtx(w, 'device', self.pmap, None)
         w("static pm_arena pm_ws_arena;")
         w("static pm_arena pm_ctab_arena;")
         w("")
@@ -671,8 +767,8 @@ class PipelineGen(object):
         w("void* ws = nullptr;")
         w("if ((st = pm_arena_get(&pm_ws_arena, wstotal, &ws))) return st;")
         w("A.ws = (char*)ws;")
-        for fnm in launches:
-            w("if ((st = %s(A, wsoff, s))) return st;" % fnm)
+        self.emit_calls(w, ["%s(A, wsoff, {s})" % f for f in self.launch_fns],
+                        "return st;")
         w("return PM_OK;")
         w.close()
         w("")
@@ -1146,9 +1242,9 @@ class PipelineGen(object):
                " && pm_batch_arena.ptr[dev] == pm_batch_ws && "
                "pm_batch_tables_current())")
         w("int st = 0;")
-        for fnm in self.batch_fns:
-            w("if ((st = %s(nullptr, nullptr, 0, n, nullptr, nullptr, nullptr, "
-              "s, 1))) return pm_status = st;" % fnm)
+        self.emit_calls(w, ["%s(nullptr, nullptr, 0, n, nullptr, nullptr, "
+                            "nullptr, {s}, 1)" % f for f in self.batch_fns],
+                        "return pm_status = st;")
         w("return pm_status = PM_OK;")
         w.close()
         w("pm_batch_key.clear(); pm_batch_ws = nullptr;")
@@ -1193,10 +1289,13 @@ class PipelineGen(object):
         w("pm_batch_pinned_cap = descs_bytes;")
         w.close()
         w("size_t doff = 0; int st = 0;")
-        for fnm in self.batch_fns:
-            w("if ((st = %s(As.data(), wsoffs.data(), %d, n, pm_batch_pinned, "
-              "ddesc, &doff, s, 0))) return pm_status = st;" % (
-                  fnm, max(self.nslots, 1)))
+        self.emit_calls(w, ["%s(As.data(), wsoffs.data(), %d, n, "
+                            "pm_batch_pinned, ddesc, &doff, {s}, 0)" % (
+                                f, max(self.nslots, 1))
+                            for f in self.batch_fns],
+                        "return pm_status = st;")
+        w("// the pinned descriptors are free once every stream's upload is")
+        w("cudaEventRecord(pm_batch_event, s);")
         w("pm_batch_key = key; pm_batch_ws = ws;")
         w("return pm_status = PM_OK;")
         w.close()
@@ -3073,14 +3172,26 @@ def generate_code_for_pipeline(pipeline):
     pg_w = pg.w
     pg.w = body
     # generate groups into `body` first so helper declarations can precede
+    pg.launch_rw = []
+    pg.launch_main = []
+    pg.conc_streams = 0
+    pg.conc_events = 0
     for g in pipeline.groups:
         plan = g.plan
+        n0 = len(pg.launch_fns)
         if plan.kind == 'stencil':
             StencilGen(pg, g).generate()
         elif plan.kind == 'reduction':
             ReductionGen(pg, g).generate()
         else:
             ConstGen(pg, g).generate()
+            # const tables are computed and uploaded on the host, in
+            # program order on the caller's stream
+            pg.launch_main.append(n0)
+        if len(pg.launch_fns) != n0 + 1:
+            raise CodegenError("group %s: expected one launch" % (
+                [c.func.name for c in g.comps],))
+        pg.launch_rw.append(pg.group_rw(g))
     pg.w = pg_w
     w = pg.w
     w("// pipeline %s -- generated by polymage_b200 for sm_100a" %
@@ -3130,7 +3241,34 @@ def generate_code_for_pipeline(pipeline):
       "192 * %d; }" % (" + ".join(pg.desc_sizes) or "0",
                        len(pg.desc_sizes) + 1))
     w("")
+    ent = W()
+    pg.w = ent
     pg.gen_entries()
+    pg.w = w
+    if pg.conc_streams:
+        # per device: side streams and events of the concurrent schedule
+        w("static cudaStream_t pm_side_stream[64][%d];" % pg.conc_streams)
+        w("static cudaEvent_t pm_conc_event[64][%d];" % pg.conc_events)
+        w.open("static int pm_conc_get(cudaStream_t* ss, int nside, int nev, "
+               "cudaEvent_t** ev)")
+        w("int dev = 0;")
+        w("if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) "
+          "return PM_ERR_CUDA;")
+        w.open("for (int k = 0; k < nside; ++k)")
+        w("if (!pm_side_stream[dev][k] && cudaStreamCreateWithFlags("
+          "&pm_side_stream[dev][k], cudaStreamNonBlocking) != cudaSuccess) "
+          "return PM_ERR_CUDA;")
+        w("ss[k + 1] = pm_side_stream[dev][k];")
+        w.close()
+        w("for (int e = 0; e < nev; ++e)")
+        w("  if (!pm_conc_event[dev][e] && cudaEventCreateWithFlags("
+          "&pm_conc_event[dev][e], cudaEventDisableTiming) != cudaSuccess) "
+          "return PM_ERR_CUDA;")
+        w("*ev = pm_conc_event[dev];")
+        w("return PM_OK;")
+        w.close()
+        w("")
+    w.lines.extend(ent.lines)
     header = pg.gen_header()
     return CudaModule(pipeline.name, w.text(), pg.host_text(), header,
                       pg.meta)
