@@ -9,7 +9,13 @@ inside blury (a larger inline budget) on 128x128 tiles, also outside the
 tuned space: with 16-byte shared-memory reads the recomputation is cheaper
 than a second shared-memory stage and its barrier (0.087-0.090 vs
 0.094 ms for the tuned best).  The camera pipe fuses with group size 12
-(one group more than the tuned best at 9: 0.197 vs 0.211 ms)."""
+(one group more than the tuned best at 9: 0.197 vs 0.211 ms).  Harris,
+the camera pipe and both pyramids ask ptxas for 4 resident CTAs per SM
+(``min_blocks=4``: at most 64 registers a thread), also outside the tuned
+space: 0.0290 vs 0.0303 ms, 0.185 vs 0.195 ms, 0.203 vs 0.209 ms and
+0.218 vs 0.227 ms (the 8-level pyramid with its interior tiles reading
+clamped taps unclamped); the bilateral grid is slower with it (0.108 vs
+0.107 ms) and unsharp is bound by shared memory, not registers."""
 
 import functools
 
@@ -19,16 +25,19 @@ from .campipe import build_campipe
 from .bilateral_grid import build_bilateral
 from .pyramid_blend import build_pyramid, build_pyramid_clamped
 
-HARRIS = dict(tile_sizes=(16, 128), group_size=11, options=('rblock=8',))
+HARRIS = dict(tile_sizes=(16, 128), group_size=11,
+              options=('rblock=8', 'min_blocks=4'))
 UNSHARP = dict(tile_sizes=(128, 128), group_size=10,
                options=('rblock=8', 'inline_budget=400'))
-CAMPIPE = dict(tile_sizes=(32, 64), group_size=12, options=('rblock=8',))
+CAMPIPE = dict(tile_sizes=(32, 64), group_size=12,
+               options=('rblock=8', 'min_blocks=4'))
 BILATERAL = dict(tile_sizes=(1, 32, 128), group_size=10,
                  options=(('red_tile', (32, 256)), 'rblock=4'))
-PYRAMID = dict(tile_sizes=(32, 64), group_size=10, options=('rblock=8',))
+PYRAMID = dict(tile_sizes=(32, 64), group_size=10,
+               options=('rblock=8', 'min_blocks=4'))
 # 8 levels, indices clamped at every level's borders (any image size)
 PYRAMID8 = dict(L=8, tile_sizes=(32, 64), group_size=10,
-                options=('rblock=8',))
+                options=('rblock=8', 'min_blocks=4'))
 
 _BUILDERS = {
     "harris": (build_harris, HARRIS),

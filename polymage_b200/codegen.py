@@ -65,7 +65,7 @@ from .expression import substitute_vars, getType, affine_form
 from .bounds import part_boxes
 from .pipe import body_parts
 from .tiling import IndexFn, is_data_dependent
-from .evaluate import monotone_dir
+from .evaluate import monotone_dir, is_min_max
 
 _INT_T = (C.Int, C.UInt, C.Short, C.UShort, C.Char, C.UChar, C.Long,
           C.ULong)
@@ -175,6 +175,11 @@ class ExprCtx(object):
         # (C name -> (residue, modulus)), for folding x % k and parity
         # Selects on interior tiles
         self.var_res = {}
+        # interior tiles whose clamped indices provably do not clamp: a
+        # min/max of an index with a bound free of loop variables prints
+        # as its unclamped arm (only inside index expressions)
+        self.fold_clamps = False
+        self._in_index = 0
 
     def temp(self):
         self.ntemp += 1
@@ -254,6 +259,10 @@ class ExprCtx(object):
         if isinstance(e, C.Cast):
             return "((%s)(%s))" % (ctype(e.typ), self.expr(e.expression, bind))
         if isinstance(e, C.Select):
+            if self.fold_clamps and self._in_index:
+                arm = _clamp_arm(e)
+                if arm is not None:
+                    return self.expr(arm, bind)
             sv = self._static_cond(e.condition, bind)
             if sv is not None:
                 # the condition is known here: only the taken arm is
@@ -365,6 +374,32 @@ class ExprCtx(object):
 
     def index(self, e):
         """Canonical C text of an index AST over loop variables."""
+        saved = self._in_index
+        # clamps fold only in an index monotone in one loop variable and
+        # free of data: the indices whose clamps the interior test checks
+        self._in_index = 0
+        if self.fold_clamps and not is_data_dependent(e):
+            vs = dict((id(v), v) for v in e.collect(C.Variable)
+                      if not isinstance(v, C.Parameter))
+            if len(vs) == 1 and monotone_dir(
+                    e, list(vs.values())[0]) in (1, -1):
+                self._in_index = 1
+        try:
+            return self._index(e)
+        finally:
+            self._in_index = saved
+
+    def unclamped(self, e, bind):
+        """C text of index ``e`` with its clamps (min/max against bounds
+        free of loop variables) dropped."""
+        saved = (self.fold_clamps, self._in_index)
+        self.fold_clamps, self._in_index = True, 1
+        try:
+            return self.expr(e, bind)
+        finally:
+            self.fold_clamps, self._in_index = saved
+
+    def _index(self, e):
         f = affine_form(e)
         if f is not None:
             parts = []
@@ -391,6 +426,36 @@ def _opt(pipeline, name, default=None):
 
 def _vn(v):
     return "v_" + re.sub(r'[^A-Za-z0-9_]', '_', v.name)
+
+
+def _has_loop_var(e):
+    return any(not isinstance(v, C.Parameter)
+               for v in e.collect(C.Variable))
+
+
+def _clamp_arm(e):
+    """The unclamped arm of a clamp ``min/max(v, bound)`` in index
+    arithmetic (``bound`` free of loop variables, no data), else None."""
+    if not is_min_max(e) or is_data_dependent(e):
+        return None
+    t, f = e.true_expression, e.false_expression
+    tv, fv = _has_loop_var(t), _has_loop_var(f)
+    if tv and not fv:
+        return t
+    if fv and not tv:
+        return f
+    return None
+
+
+def _has_clamp(e):
+    stack = [e]
+    while stack:
+        n = stack.pop()
+        if _clamp_arm(n) is not None:
+            return True
+        if hasattr(n, 'children'):
+            stack.extend(n.children())
+    return False
 
 
 def _subst(a, bind):
@@ -1421,6 +1486,7 @@ class StencilGen(object):
         self.clamp = False
         self.inside = False
         self.has_inside = False
+        self.fold_ok = False
         self.g = group
         self.plan = group.plan
         self.k = "pm_%s_g%d" % (pg.pname, group.level_time)
@@ -1565,8 +1631,12 @@ class StencilGen(object):
         anchor = plan.anchor
         na = anchor.ndims
         nt = plan.threads
-        w('extern "C" __global__ void __launch_bounds__(%d) %s(const '
-          '__grid_constant__ %s_launch L)' % (nt, k, k))
+        # option 'min_blocks=N': ask ptxas for N resident CTAs per SM
+        # (caps registers per thread)
+        mb = int(_opt(pg.p, 'min_blocks', 0) or 0)
+        lb = "%d, %d" % (nt, mb) if mb > 0 else "%d" % nt
+        w('extern "C" __global__ void __launch_bounds__(%s) %s(const '
+          '__grid_constant__ %s_launch L)' % (lb, k, k))
         w.open("")
         w("extern __shared__ __align__(128) unsigned char pm_smem[];")
         if self.stage_nodes:
@@ -1725,9 +1795,33 @@ class StencilGen(object):
         inside = self.inside_conds()
         self.has_inside = inside is not None and \
             'no_inside' not in pg.p.options
+        # clamped indices (min/max against bounds free of loop variables)
+        # that do not clamp at either end of their consumer's region do
+        # not clamp anywhere in it (the clamp is monotone in a monotone
+        # index): interior tiles then read them unclamped
+        unclamp = []
+        if 'no_fold_clamps' not in pg.p.options:
+            for n in plan.nodes:
+                for m, per_dim in self.distinct_uses(n):
+                    mn = self.node_name(m)
+                    for fns in per_dim:
+                        for fn in fns:
+                            if fn.kind != 'mono' or not _has_clamp(fn.expr):
+                                continue
+                            for end in ("lo", "hi"):
+                                b = {fn.var: "r_%s_%s%d" % (mn, end,
+                                                            fn.cdim)}
+                                c = "(%s) == (%s)" % (ctx.expr(fn.expr, b),
+                                                      ctx.unclamped(fn.expr,
+                                                                    b))
+                                if c not in unclamp:
+                                    unclamp.append(c)
+        self.fold_ok = bool(unclamp)
         if self.has_inside:
+            # the clamp checks come last: && evaluates them only on tiles
+            # whose regions are full (no overflow on empty regions)
             w("const bool pm_inside = %s;" % (
-                " && ".join(conds + inside) or "true"))
+                " && ".join(conds + inside + unclamp) or "true"))
 
     def effective_bounds(self, n):
         """Bounds of the points of a node that read their producers: the
@@ -2196,9 +2290,11 @@ class StencilGen(object):
             if self.has_inside:
                 w.open("if (pm_inside)")
                 self.fast = self.inside = True
+                self.ctx.fold_clamps = self.fold_ok
                 self.vec = self.choose_vec(f, n, ext)
                 self.gen_fast_loop(f, n, ext)
                 self.vec = 1
+                self.ctx.fold_clamps = False
                 self.fast = self.inside = False
                 w.close()
                 w.open("else")

@@ -53,3 +53,28 @@ def test_pyramid8_batch_graph(cp, cuda):
             err = np.abs(o['blend'].cpu().numpy().astype(np.float64) -
                          ref).max()
             assert err <= 2e-5, err
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_pyramid8_joins_the_callers_stream(cp, cuda, graph):
+    """The groups run on several streams; the call's stream must follow
+    all of them: a copy queued on that stream right after the call, with
+    no device synchronization in between, sees the finished output."""
+    import torch
+    R, C = 1500, 1700
+    img1, img2, mask = OP.make_inputs(R, C, seed=9)
+    ref = OP.pyramid_blend_clamped(img1, img2, mask, L=8)
+    ins = {'img1': torch.from_numpy(img1).to(cuda),
+           'img2': torch.from_numpy(img2).to(cuda),
+           'mask': torch.from_numpy(mask).to(cuda)}
+    side = torch.cuda.Stream(cuda)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(side):
+        for _ in range(3):
+            out = torch.zeros((3, R, C), dtype=torch.float32, device=cuda)
+            cp.run_dev({'R': R, 'C': C}, ins, {'blend': out}, graph=graph)
+            snap = out.clone()
+        side.synchronize()
+    cp.check()
+    err = np.abs(snap.cpu().numpy().astype(np.float64) - ref).max()
+    assert err <= 2e-5, err
