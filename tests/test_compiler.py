@@ -143,3 +143,32 @@ def test_level_size_divisions_do_not_enter_the_period():
     assert plan.period == 1
     ext = dict((n.name, n.ext) for n in plan.nodes)
     assert ext['a'] == [67, 64]
+
+
+def test_interior_tiles_check_clamps_before_reading_unclamped():
+    """A clamped tap is read unclamped on interior tiles only: the
+    interior test compares each clamped index with its unclamped form at
+    both ends of the consumer's region.  Data-dependent clamps (a LUT
+    index) are never dropped."""
+    R = Parameter(Int, "R")
+    C = Parameter(Int, "C")
+    x = Variable(Int, "x")
+    y = Variable(Int, "y")
+    img = Image(Float, "img", [R, C])
+    lut = Image(Float, "lut", [256])
+    a = Function(([x, y], [Interval(Int, 0, R - 1), Interval(Int, 0, C - 1)]),
+                 Float, "a")
+    a.defn = [sum(img(Min(Max(x + k - 1, 0), R - 1), y) for k in range(3))]
+    b = Function(([x, y], [Interval(Int, 0, R - 1), Interval(Int, 0, C - 1)]),
+                 Float, "b")
+    b.defn = [lut(Min(Max(Cast(Int, a(x, y) * 64.0), 0), 255))]
+    p = buildPipeline([b], param_estimates=[(R, 1024), (C, 1024)],
+                      tile_sizes=[32, 64], group_size=2)
+    src = p.generate_code().source
+    inside = [ln for ln in src.splitlines() if 'const bool pm_inside' in ln]
+    assert inside and all(') == (' in ln for ln in inside)
+    fast = src[src.index('if (pm_inside)'):]
+    fast = fast[:fast.index('} else {') if '} else {' in fast else None]
+    # the image taps read unclamped; the LUT index keeps its clamp
+    assert 'sm_img[(qb0 - 1) * ' in fast
+    assert '< 255) ?' in fast
