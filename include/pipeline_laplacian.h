@@ -1,0 +1,28 @@
+/* pipeline_laplacian -- C ABI of the PolyMage pipeline 'laplacian' built for NVIDIA B200 (sm_100a).
+ * Generated by polymage_b200; argument order: parameters, then inputs, then
+ * outputs, each sorted by name (the reference's generated pipeline_<name> ABI). */
+#pragma once
+#ifdef __cplusplus
+extern "C" {
+#endif
+/* host buffers, synchronous (reference ABI) */
+void pipeline_laplacian(int C, int R, float alpha, float beta, void* img_colour, void* laplacian);
+/* device buffers, asynchronous on `stream` (cudaStream_t); returns a PM status */
+int pipeline_laplacian_dev(int C, int R, float alpha, float beta, void* img_colour, void* laplacian, void* stream);
+/* same as _dev through a CUDA graph captured on first use */
+int pipeline_laplacian_graph(int C, int R, float alpha, float beta, void* img_colour, void* laplacian, void* stream);
+/* n images; iparams: n x 2 int params, fparams: n x 2 float params, each row in
+ * name order; inputs: n x 1 device pointers, outputs: n x 1 device pointers */
+int pipeline_laplacian_batch(int n, const int* iparams, const float* fparams, void* const* inputs, void* const* outputs, void* stream);
+/* same as _batch through a CUDA graph captured on first use (re-captured when
+ * the arguments change); a repeated _batch call with unchanged arguments
+ * relaunches kernels only */
+int pipeline_laplacian_batch_graph(int n, const int* iparams, const float* fparams, void* const* inputs, void* const* outputs, void* stream);
+/* status of the last call: 0 ok, 1 bad parameters, 2 CUDA error, 3 kernel error */
+int pipeline_laplacian_status(void);
+/* synchronizes and reports the device error word */
+int pipeline_laplacian_check(void);
+void pipeline_laplacian_clear_error(void);
+#ifdef __cplusplus
+}
+#endif

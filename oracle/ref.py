@@ -9,6 +9,10 @@ infrastructure only (parity pinning and the CPU baseline).
   float weight, void* uint8 [R+4][C+4][3], void* float [R][C][3])``
   (sandbox/video_demo/unsharp_polymage.cpp:10-99): unsharp mask over the
   whole image (no Case), interleaved uint8 input scaled by 1/255.
+* ``ref_laplacian``: ``pipeline_laplacian(int C, int R, float alpha,
+  float beta, void* uint8 [R-92][C-92][3], void* uint8 [R-92][C-92][3])``
+  (sandbox/video_demo/laplacian_polymage.cpp:10-1062): the local
+  Laplacian filter of the video demo, frame padded internally.
 """
 
 import ctypes
@@ -73,6 +77,22 @@ def ref_unsharp(img_u8, threshold, weight, out=None):
                    ctypes.c_void_p, ctypes.c_void_p]
     fn.restype = None
     fn(C, R, float(threshold), float(weight), img_u8.ctypes.data,
+       out.ctypes.data)
+    return out
+
+
+def ref_laplacian(frame_u8, alpha, beta, out=None):
+    """frame_u8: uint8 [rows][cols][3] -> uint8 [rows][cols][3]."""
+    frame_u8 = np.ascontiguousarray(frame_u8, dtype=np.uint8)
+    H, W, _ = frame_u8.shape
+    if out is None:
+        out = np.zeros((H, W, 3), np.uint8)
+    lib = _lib("laplacian")
+    fn = lib.pipeline_laplacian
+    fn.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                   ctypes.c_void_p, ctypes.c_void_p]
+    fn.restype = None
+    fn(W + 92, H + 92, float(alpha), float(beta), frame_u8.ctypes.data,
        out.ctypes.data)
     return out
 

@@ -24,6 +24,7 @@ from .unsharp_mask import build_unsharp
 from .campipe import build_campipe
 from .bilateral_grid import build_bilateral
 from .pyramid_blend import build_pyramid, build_pyramid_clamped
+from .local_laplacian import build_laplacian
 
 HARRIS = dict(tile_sizes=(16, 128), group_size=11,
               options=('rblock=8', 'min_blocks=4'))
@@ -39,6 +40,9 @@ PYRAMID = dict(tile_sizes=(32, 64), group_size=10,
 PYRAMID8 = dict(L=8, tile_sizes=(32, 64), group_size=10,
                 options=('rblock=8', 'min_blocks=4'))
 
+# local Laplacian filter (the video demo's pipeline_laplacian), 1080p frames
+LAPLACIAN = dict(tile_sizes=(32, 64), group_size=10, options=('rblock=8',))
+
 _BUILDERS = {
     "harris": (build_harris, HARRIS),
     "unsharp": (build_unsharp, UNSHARP),
@@ -46,6 +50,7 @@ _BUILDERS = {
     "bilateral": (build_bilateral, BILATERAL),
     "pyramid": (build_pyramid, PYRAMID),
     "pyramid8": (build_pyramid_clamped, PYRAMID8),
+    "laplacian": (build_laplacian, LAPLACIAN),
 }
 
 _cache = {}

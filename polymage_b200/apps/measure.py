@@ -21,7 +21,8 @@ import numpy as np
 
 from . import catalog
 
-APPS = ("harris", "unsharp", "campipe", "bilateral", "pyramid", "pyramid8")
+APPS = ("harris", "unsharp", "campipe", "bilateral", "pyramid", "pyramid8",
+        "laplacian")
 FLUSH_BYTES = 256 << 20
 
 
@@ -75,6 +76,14 @@ def workload(app, seed=0):
                  'mask': rng.random((R, C), dtype=np.float32)},
                 {'blend': ((3, R, C), np.float32)}, R * C,
                 "pyramid_blend L=8 (clamped borders) 3x2048x2048 float32")
+    if app == 'laplacian':
+        H, W = 1080, 1920
+        return ({'R': H + 92, 'C': W + 92, 'alpha': 1.0 / 3.0, 'beta': 1.0},
+                {'img_colour': rng.integers(0, 256, (H, W, 3),
+                                            dtype=np.uint8)},
+                {'laplacian': ((H, W, 3), np.uint8)}, H * W,
+                "local_laplacian 1920x1080 uint8 BGR, 4 intensity levels, "
+                "5 pyramid levels")
     raise ValueError(app)
 
 

@@ -7,6 +7,9 @@ harris.npz   refHarris (sandbox/ipp_bench/harris/harris_function.cpp) on a
              40x56 float32 image, U[0,1) seed 123
 unsharp.npz  pipeline_mask (sandbox/video_demo/unsharp_polymage.cpp) on a
              (24+4)x(37+4)x3 uint8 image, seed 321, threshold 0.001, w 3
+laplacian.npz  pipeline_laplacian (sandbox/video_demo/laplacian_
+             polymage.cpp) on 64x96x3 and 75x131x3 uint8 frames, seeds 7
+             and 8, alpha 1/3, beta 1 (the video demo's settings)
 """
 
 import os
@@ -30,7 +33,16 @@ def main():
     out = ref.ref_unsharp(u8, 0.001, 3.0)
     np.savez_compressed(os.path.join(HERE, "unsharp.npz"), img=u8, out=out,
                         threshold=np.float32(0.001), weight=np.float32(3.0))
-    print("wrote harris.npz, unsharp.npz")
+    arrs = {}
+    for n, (seed, h, w) in enumerate(((7, 64, 96), (8, 75, 131))):
+        frame = np.random.default_rng(seed).integers(0, 256, (h, w, 3),
+                                                     dtype=np.uint8)
+        arrs['frame%d' % n] = frame
+        arrs['out%d' % n] = ref.ref_laplacian(frame, 1.0 / 3.0, 1.0)
+    np.savez_compressed(os.path.join(HERE, "laplacian.npz"),
+                        alpha=np.float32(1.0 / 3.0), beta=np.float32(1.0),
+                        **arrs)
+    print("wrote harris.npz, unsharp.npz, laplacian.npz")
 
 
 if __name__ == "__main__":

@@ -58,3 +58,14 @@ def test_clamped_pyramid_oracle_matches_reference_spec_inside():
     (x0, x1), (y0, y1) = OP.output_box(R, C)
     assert ref.shape == (3, x1 - x0 + 1, y1 - y0 + 1)
     assert np.abs(gen[:, x0:x1 + 1, y0:y1 + 1] - ref).max() < 1e-12
+
+
+def test_laplacian_restatement_matches_reference_fixtures():
+    """The float32 NumPy restatement of the local Laplacian reproduces the
+    reference's compiled pipeline_laplacian exactly on the fixtures."""
+    import oracle.laplacian as OL
+    z = np.load(os.path.join(GOLD, "laplacian.npz"))
+    for n in range(2):
+        got = OL.local_laplacian(z['frame%d' % n], float(z['alpha']),
+                                 float(z['beta']))
+        assert np.array_equal(got, z['out%d' % n])
