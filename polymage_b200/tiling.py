@@ -300,14 +300,26 @@ class ConstPlan(object):
 
 
 # ---------------------------------------------------------------------------
-def _tile_sizes_for(pipeline, ndims):
+def _tile_sizes_for(pipeline, ndims, anchor=None, env=None):
+    """Tile extent per anchor dimension: the tile sizes apply to the
+    innermost dimensions, leading ones get 1.  With fewer sizes than
+    dimensions, an innermost dimension of constant extent <= 4 (the
+    channels of an interleaved image, [x][y][c]) is tiled whole and the
+    sizes go to the dimensions before it."""
     ts = list(pipeline.tile_sizes)
     opt = _option(pipeline, 'tile')
     if opt is not None:
         ts = list(opt)
     if len(ts) >= ndims:
         return [int(t) for t in ts[len(ts) - ndims:]]
-    return [1] * (ndims - len(ts)) + [int(t) for t in ts]
+    tail = []
+    if anchor is not None and env is not None and ndims > len(ts):
+        e = _const_extent(anchor.domain[ndims - 1], env)
+        if e is not None and e <= 4:
+            tail = [int(e)]
+    n = ndims - len(tail)
+    head = [int(t) for t in ts[max(0, len(ts) - n):]]
+    return [1] * (n - len(head)) + head + tail
 
 
 def _option(pipeline, name, default=None):
@@ -373,7 +385,7 @@ def plan_stencil(pipeline, comps):
     plan.threads = int(_option(pipeline, 'threads', DEFAULT_THREADS))
     budget = int(_option(pipeline, 'inline_budget', DEFAULT_INLINE_BUDGET))
     forced_smem = set(_option(pipeline, 'materialize', []) or [])
-    plan.tile = _tile_sizes_for(pipeline, anchor.ndims)
+    plan.tile = _tile_sizes_for(pipeline, anchor.ndims, anchor, env)
 
     # ---- materialization decisions, sinks first --------------------------
     uses = {}          # func -> [(M func, [arg exprs])]
