@@ -172,3 +172,17 @@ def test_interior_tiles_check_clamps_before_reading_unclamped():
     # the image taps read unclamped; the LUT index keeps its clamp
     assert 'sm_img[(qb0 - 1) * ' in fast
     assert '< 255) ?' in fast
+
+
+def test_interleaved_channels_tiled_whole():
+    """An anchor [x][y][c] with 3 interleaved channels gets tiles of
+    32 x 64 pixels x all channels, not 1 x 32 x 64 (x, y, c); planar
+    [c][x][y] anchors keep one channel per tile."""
+    from polymage_b200.apps.local_laplacian import build_laplacian
+    p = build_laplacian(rows=270, cols=480)
+    tiles = dict((g.plan.anchor.name, g.plan.tile) for g in p.groups
+                 if g.plan is not None and hasattr(g.plan, 'anchor'))
+    assert tiles['laplacian'] == [32, 64, 3]
+    assert tiles['gPyramid_L0'] == [1, 32, 64]
+    q = build_unsharp(tile_sizes=(32, 128))
+    assert q.groups[0].plan.tile == [1, 32, 128]
