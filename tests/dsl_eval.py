@@ -1,0 +1,120 @@
+"""Direct evaluation of DSL definitions, point by point, in FP64 with C
+integer semantics -- a test aid.  It reads the spec the way the reference
+defines it (later Cases override earlier ones; points no Case covers read
+as 0, the convention of the oracles) and so checks a restatement against
+the definitions it restates, independently of the compiler.  Slow:
+tiny images only."""
+
+import math
+
+import numpy as np
+
+from polymage_b200 import constructs as C
+from polymage_b200.expr_ast import (Value, AbstractBinaryOpNode,
+                                    AbstractUnaryOpNode)
+from polymage_b200.evaluate import c_div, c_mod
+from polymage_b200.pipe import body_parts
+
+_BUILTINS = {C.Exp: math.exp, C.Log: math.log, C.Sqrt: math.sqrt,
+             C.Sqrtf: math.sqrt, C.Abs: abs, C.Sin: math.sin,
+             C.Cos: math.cos, C.Pow: math.pow, C.Powf: math.pow}
+_INTS = (C.Int, C.UInt, C.Short, C.UShort, C.Char, C.UChar, C.Long,
+         C.ULong)
+
+
+class Evaluator(object):
+    def __init__(self, params, images):
+        """``params``: {name: value}; ``images``: {name: numpy array}
+        indexed from 0 (the image's domain lower bounds are 0)."""
+        self.params = params
+        self.images = images
+        self.memo = {}
+
+    def value(self, f, args):
+        args = tuple(int(a) for a in args)
+        if isinstance(f, C.Image):
+            a = self.images[f.name]
+            return a[args].item()
+        key = (id(f), args)
+        if key in self.memo:
+            return self.memo[key]
+        env = dict(zip([id(v) for v in f.variables], args))
+        v = 0
+        for cond, expr, red in body_parts(f):
+            if red is not None:
+                raise NotImplementedError("reductions")
+            if cond is None or self.cond(cond, env):
+                v = self.expr(expr, env)
+        if f.typ in _INTS:
+            v = int(v)
+        self.memo[key] = v
+        return v
+
+    def cond(self, c, env):
+        op = c.conditional
+        if op in ('&&', '||'):
+            a = self.cond(c.lhs, env)
+            if op == '&&':
+                return a and self.cond(c.rhs, env)
+            return a or self.cond(c.rhs, env)
+        a = self.expr(c.lhs, env)
+        b = self.expr(c.rhs, env)
+        return {'<': a < b, '<=': a <= b, '>': a > b, '>=': a >= b,
+                '==': a == b, '!=': a != b}[op]
+
+    def expr(self, e, env):
+        e = Value.numericToValue(e)
+        if isinstance(e, Value):
+            v = e.value
+            return int(v) if e.typ in _INTS else float(v)
+        if isinstance(e, C.Parameter):
+            return self.params[e.name]
+        if isinstance(e, C.Variable):
+            return env[id(e)]
+        if isinstance(e, C.Reference):
+            return self.value(e.objectRef, [self.expr(a, env)
+                                            for a in e.arguments])
+        if isinstance(e, AbstractBinaryOpNode):
+            a = self.expr(e.left, env)
+            b = self.expr(e.right, env)
+            ints = isinstance(a, int) and isinstance(b, int)
+            op = e.op
+            if op == '+':
+                return a + b
+            if op == '-':
+                return a - b
+            if op == '*':
+                return a * b
+            if op == '/':
+                return c_div(a, b) if ints else a / b
+            if op == '%':
+                return c_mod(a, b)
+            raise NotImplementedError(op)
+        if isinstance(e, AbstractUnaryOpNode):
+            v = self.expr(e.child, env)
+            return -v if e.op == '-' else v
+        if isinstance(e, C.Select):
+            if self.cond(e.condition, env):
+                return self.expr(e.true_expression, env)
+            return self.expr(e.false_expression, env)
+        if isinstance(e, C.Cast):
+            v = self.expr(e.expression, env)
+            return int(v) if e.typ in _INTS else float(v)
+        for cls, fn in _BUILTINS.items():
+            if isinstance(e, cls):
+                return fn(*[self.expr(a, env) for a in e.arguments])
+        raise NotImplementedError(type(e).__name__)
+
+    def array(self, f, params_shape=None):
+        """Every point of ``f``'s domain (lower bounds must be 0)."""
+        dom = []
+        for d in f.domain:
+            lo = self.expr(d.lowerBound, {})
+            hi = self.expr(d.upperBound, {})
+            dom.append((lo, hi))
+        shape = tuple(hi - lo + 1 for lo, hi in dom)
+        out = np.zeros(shape)
+        for idx in np.ndindex(*shape):
+            out[idx] = self.value(f, [i + lo for i, (lo, _) in
+                                      zip(idx, dom)])
+        return out
