@@ -186,3 +186,13 @@ def test_interleaved_channels_tiled_whole():
     assert tiles['gPyramid_L0'] == [1, 32, 64]
     q = build_unsharp(tile_sizes=(32, 128))
     assert q.groups[0].plan.tile == [1, 32, 128]
+
+
+def test_interpolate_plans_and_compiles():
+    """The 10-level interpolation (next app after the benchmark set)
+    plans into fused groups and compiles for sm_100a."""
+    from polymage_b200.apps.interpolate import build_interpolate
+    p = build_interpolate(rows=512, cols=512)
+    assert 5 <= len(p.groups) <= 20
+    cp = p.build()
+    assert cp.so_path.endswith(".so")
