@@ -38,17 +38,52 @@ class Evaluator(object):
         key = (id(f), args)
         if key in self.memo:
             return self.memo[key]
+        if isinstance(f, C.Reduction):
+            self.reduce(f)
+            return self.memo.get(key, self.expr(f.default, {}))
         env = dict(zip([id(v) for v in f.variables], args))
         v = 0
         for cond, expr, red in body_parts(f):
-            if red is not None:
-                raise NotImplementedError("reductions")
             if cond is None or self.cond(cond, env):
                 v = self.expr(expr, env)
         if f.typ in _INTS:
             v = int(v)
         self.memo[key] = v
         return v
+
+    def reduce(self, f):
+        """Every cell of a Reduction: the default, then each part's
+        ``Reduce`` applied in order over the reduction domain (sequential
+        accumulation, as the reference's generated loops do)."""
+        done = (id(f), 'reduced')
+        if done in self.memo:
+            return
+        self.memo[done] = True
+        ranges = []
+        for d in f.reductionDomain:
+            ranges.append(range(self.expr(d.lowerBound, {}),
+                                self.expr(d.upperBound, {}) + 1))
+        ids = [id(v) for v in f.reductionVariables]
+        dflt = self.expr(f.default, {})
+        ops = {C.Op.Sum: lambda a, b: a + b, C.Op.Mul: lambda a, b: a * b,
+               C.Op.Min: min, C.Op.Max: max}
+        for cond, expr, red in body_parts(f):
+            op = ops[red.op_type]
+            for pt in np.ndindex(*[len(r) for r in ranges]):
+                env = dict((i, r[k]) for i, r, k in zip(ids, ranges, pt))
+                cell = tuple(int(self.expr(a, env)) for a in
+                             red.accumulate_ref.arguments)
+                # a function variable that is not reduced over stands for
+                # the target cell's index (a condition on it selects cells)
+                for fv, ci in zip(f.variables, cell):
+                    if id(fv) not in env:
+                        env[id(fv)] = ci
+                if cond is not None and not self.cond(cond, env):
+                    continue
+                key = (id(f), cell)
+                cur = self.memo.get(key, dflt)
+                v = op(cur, self.expr(expr, env))
+                self.memo[key] = int(v) if f.typ in _INTS else v
 
     def cond(self, c, env):
         op = c.conditional

@@ -44,3 +44,68 @@ def test_interpolate_restatement_matches_statement():
         ev = Evaluator({'R': R, 'C': C}, {'img': img.astype(np.float64)})
         got = ev.array(interpolate({}))
         assert np.abs(got - OI.interpolate(img)).max() <= 1e-12
+
+
+def test_unsharp_statement_matches_pinned_oracle():
+    import oracle.unsharp as OU
+    from polymage_b200.apps.unsharp_mask import unsharp_mask
+    R, C = 12, 17
+    img = OU.make_input(R, C, seed=3)
+    ev = Evaluator({'R': R, 'C': C, 'threshold': 0.001, 'weight': 3.0},
+                   {'img': img.astype(np.float64)})
+    got = ev.array(unsharp_mask({}))
+    ok = OU.margin(img, 0.001) > 1e-6
+    assert np.abs(got - OU.unsharp(img, 0.001, 3.0))[ok].max() <= 1e-12
+
+
+def test_pyramid_statements_match_oracles():
+    import oracle.pyramid as OP
+    from polymage_b200.apps.pyramid_blend import (pyramid_blending,
+                                                  pyramid_blending_clamped)
+    R, C = 96, 100
+    i1, i2, m = OP.make_inputs(R, C, seed=1)
+    imgs = {'img1': i1.astype(np.float64), 'img2': i2.astype(np.float64),
+            'mask': m.astype(np.float64)}
+    got = Evaluator({'R': R, 'C': C}, imgs).array(pyramid_blending({}))
+    assert np.abs(got - OP.pyramid_blend(i1, i2, m)).max() <= 1e-12
+    R, C = 37, 53
+    i1, i2, m = OP.make_inputs(R, C, seed=2)
+    imgs = {'img1': i1.astype(np.float64), 'img2': i2.astype(np.float64),
+            'mask': m.astype(np.float64)}
+    got = Evaluator({'R': R, 'C': C}, imgs).array(
+        pyramid_blending_clamped({}, L=8))
+    ref = OP.pyramid_blend_clamped(i1, i2, m, L=8)
+    assert np.abs(got - ref).max() <= 1e-12
+
+
+def test_bilateral_statement_matches_oracle():
+    """The grid is a Reduction: accumulated sequentially over the image;
+    the oracle bins z in float32 (as the kernel does), the evaluator in
+    FP64, hence the tolerance."""
+    import oracle.bilateral as OB
+    from polymage_b200.apps.bilateral_grid import bilateral_grid
+    rows, cols = 40, 48
+    img = OB.make_input(rows, cols, seed=5)
+    got = Evaluator({'rows': rows, 'cols': cols},
+                    {'input': img.astype(np.float64)}).array(
+        bilateral_grid({}))
+    assert np.abs(got - OB.bilateral(img)).max() <= 1e-6
+
+
+def test_campipe_statement_matches_c_restatement():
+    """Integer pipeline; the evaluator computes the const LUT in FP64 where
+    the restatement uses the reference's float/double mix, so an entry may
+    round differently: at most one count on at most 1 % of the bytes."""
+    import oracle.campipe as OC
+    from polymage_b200.apps.campipe import (camera_pipe, MATRIX_3200,
+                                            MATRIX_7000)
+    R, C = 80, 96
+    img = OC.make_input(R, C, seed=4)
+    ev = Evaluator({'R': R, 'C': C, 'colour_temp': 3700.0, 'contrast': 50.0,
+                    'gamma': 2.0},
+                   {'img': img.astype(np.int64),
+                    'matrix_3200': np.array(MATRIX_3200),
+                    'matrix_7000': np.array(MATRIX_7000)})
+    got = ev.array(camera_pipe({}))
+    d = np.abs(got - OC.campipe(img, 3700.0, 50.0, 2.0).astype(np.float64))
+    assert d.max() <= 1 and (d > 0).mean() <= 0.01
