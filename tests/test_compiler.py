@@ -196,3 +196,62 @@ def test_interpolate_plans_and_compiles():
     assert 5 <= len(p.groups) <= 20
     cp = p.build()
     assert cp.so_path.endswith(".so")
+
+
+def _tile_boxes(plan, env):
+    """Every tile of a group's grid, as the kernel enumerates them: the
+    union of its live-outs' domains along the anchor dimensions, cut into
+    tiles of the plan's sizes."""
+    import itertools
+    from polymage_b200.evaluate import eval_int
+    na = plan.anchor.ndims
+    lo = [None] * na
+    hi = [None] * na
+    for n in plan.nodes:
+        if n.role != 'out':
+            continue
+        for d, dom in enumerate(n.func.domain):
+            k = d if n.func is plan.anchor else n.owned_map[d]
+            a, b = eval_int(dom.lowerBound, env), eval_int(dom.upperBound, env)
+            lo[k] = a if lo[k] is None else min(lo[k], a)
+            hi[k] = b if hi[k] is None else max(hi[k], b)
+    starts = [range(lo[k], hi[k] + 1, plan.tile[k]) for k in range(na)]
+    for origin in itertools.product(*starts):
+        yield [(o, min(o + t - 1, h)) for o, t, h in
+               zip(origin, plan.tile, hi)]
+
+
+@pytest.mark.parametrize("name,sizes", [
+    ("pyramid8", (256, 300)), ("pyramid8", (37, 53)),
+    ("pyramid", (157, 211)), ("campipe", (200, 264)),
+    ("laplacian", (64 + 92, 96 + 92)), ("bilateral", (77, 93))])
+def test_static_extents_cover_every_tile_of_every_group(name, sizes):
+    """Region inference for every tile of every fused group of a shipped
+    pipeline at a small size: each materialized node's region fits the
+    static shared-memory extents the kernel was generated with (a region
+    larger than its buffer would read or write out of it)."""
+    from polymage_b200.apps import catalog
+    b, kw = catalog._BUILDERS[name]
+    p = b(**kw)
+    env = p.int_env()
+    for k in list(env):
+        if k.name in ('R', 'rows'):
+            env[k] = sizes[0]
+        elif k.name in ('C', 'cols'):
+            env[k] = sizes[1]
+    checked = 0
+    for g in p.groups:
+        plan = g.plan
+        if getattr(plan, 'kind', None) != 'stencil':
+            continue
+        for box in _tile_boxes(plan, env):
+            regs = infer_regions(plan, box, env)
+            for n in plan.nodes:
+                if not n.in_smem:
+                    continue
+                lo, hi = regs[n.func]
+                for d in range(n.ndims):
+                    ext = int(hi[d]) - int(lo[d]) + 1
+                    assert ext <= n.ext[d], (n.name, d, ext, n.ext[d], box)
+            checked += 1
+    assert checked > 0
