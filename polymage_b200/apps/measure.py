@@ -97,7 +97,12 @@ def hbm_peak():
     return 6650.0, "fallback"
 
 
-def measure(app, steps=50, warmup=5, device=None, graph=True):
+def measure(app, steps=50, warmup=5, device=None, graph=True, warm=False):
+    """Mean device time of ``steps`` runs of one shipped pipeline at its
+    benchmark size (CUDA events on the launching stream).  By default 256 MB
+    are written before each run so that nothing starts in L2; ``warm``
+    leaves the previous run's data in L2 (the sub-L2 workloads' warm
+    numbers)."""
     import torch
     dev = device or torch.device("cuda", torch.cuda.current_device())
     cp = catalog.build(app)
@@ -123,7 +128,8 @@ def measure(app, steps=50, warmup=5, device=None, graph=True):
     ev = [(torch.cuda.Event(enable_timing=True),
            torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     for i in range(steps):
-        flush.fill_(float(i))
+        if not warm:
+            flush.fill_(float(i))
         ev[i][0].record(stream)
         cp.run_dev(prm, ins, outs, stream=stream.cuda_stream, graph=graph)
         ev[i][1].record(stream)
@@ -141,7 +147,8 @@ def measure(app, steps=50, warmup=5, device=None, graph=True):
             "entry": "pipeline_%s_%s" % (cp.name, "graph" if graph else "dev"),
             "compulsory_bytes": int(nbytes), "achieved_gbs": gbs,
             "hbm_frac": gbs / peak, "peak_gbs": peak, "peak_source": kind,
-            "l2": "256 MB written before each timed run"}
+            "l2": ("warm: the previous run's data left in L2" if warm else
+                   "256 MB written before each timed run")}
 
 
 def measure_bilateral_batch(n=64, steps=10, warmup=3, graph=True,
@@ -226,6 +233,8 @@ def main():
                     choices=APPS + ("bilateral_batch64", "stream1024"))
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--warm", action="store_true",
+                    help="no L2 flush between runs (single-image pipelines)")
     args = ap.parse_args()
     for app in args.app or APPS + ("bilateral_batch64", "stream1024"):
         if app == "stream1024":
@@ -234,7 +243,8 @@ def main():
             print(json.dumps(measure_bilateral_batch(
                 64, steps=min(args.steps, 10), warmup=args.warmup)))
         else:
-            print(json.dumps(measure(app, args.steps, args.warmup)))
+            print(json.dumps(measure(app, args.steps, args.warmup,
+                                     warm=args.warm)))
 
 
 if __name__ == "__main__":
