@@ -432,6 +432,50 @@ class Pipeline(object):
                 lines.extend("    " + l for l in g.plan.describe())
         return "\n".join(lines)
 
+    @property
+    def pipeline_graph(self):
+        """The grouped stage graph (``draw_pipeline_graph``), as the
+        reference's tests read it (sandbox/tests/test_grouping.py:47)."""
+        return self.draw_pipeline_graph()
+
+    def draw_pipeline_graph(self):
+        """The stage graph with its fused groups (the reference's
+        ``Pipeline.draw_pipeline_graph``, sandbox/pipe.py:901-932): one box
+        per stage, bold for live-outs and filled otherwise, coloured by
+        HBM storage slot; one dashed cluster per group labelled with its
+        launch order; an edge from each producer to each consumer.
+        Returned as a ``PipelineGraph`` whose ``string()`` is Graphviz DOT
+        text and ``write(path)`` writes it (the reference returns a
+        pygraphviz graph with the same two methods)."""
+        slot = getattr(self, '_storage_assign', {})
+        palette = ("lightblue", "lightpink", "palegreen", "khaki",
+                   "lightsalmon", "plum", "lightcyan", "wheat",
+                   "lightgrey", "aquamarine", "thistle", "peachpuff")
+        q = lambda n: '"%s"' % n.replace('"', r'\"')
+        lines = ["digraph %s {" % q(self._name), "  compound=true;"]
+        for i, g in enumerate(self._groups):
+            lines.append("  subgraph %s {" % q("cluster_%d" % i))
+            lines.append('    label=%s; style="dashed, rounded";' % q(
+                "%d: %s [%s]" % (getattr(g, 'level_time', i), g.name,
+                                 g.kind)))
+            for c in g.comps:
+                live = c.is_output or any(ch not in g.comps
+                                          for ch in c.children)
+                style = "rounded, bold" if live else "rounded, filled"
+                attrs = ['shape=box', 'style="%s"' % style]
+                if c in slot:
+                    attrs.append('color=%s' % palette[slot[c] %
+                                                      len(palette)])
+                lines.append("    %s [%s];" % (q(c.func.name),
+                                               ", ".join(attrs)))
+            lines.append("  }")
+        for c in self._comps:
+            for pc in c.parents:
+                lines.append("  %s -> %s;" % (q(pc.func.name),
+                                              q(c.func.name)))
+        lines.append("}")
+        return PipelineGraph("\n".join(lines) + "\n")
+
     # ---- code generation and build ----------------------------------------
     def generate_code(self, is_extern_c_func=True, are_io_void_ptrs=True):
         """The CUDA translation unit for this pipeline.  The flags are
@@ -444,3 +488,17 @@ class Pipeline(object):
         """Generate, compile (nvcc, sm_100a) and load the pipeline."""
         from .build import build_pipeline
         return build_pipeline(self, out_dir=out_dir, verbose=verbose)
+
+
+class PipelineGraph(object):
+    """Graphviz DOT text of a pipeline's stage graph."""
+
+    def __init__(self, text):
+        self._text = text
+
+    def string(self):
+        return self._text
+
+    def write(self, path):
+        with open(path, "w") as f:
+            f.write(self._text)

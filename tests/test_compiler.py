@@ -255,3 +255,21 @@ def test_static_extents_cover_every_tile_of_every_group(name, sizes):
                     assert ext <= n.ext[d], (n.name, d, ext, n.ext[d], box)
             checked += 1
     assert checked > 0
+
+
+def test_pipeline_graph_dot(tmp_path):
+    """The stage graph as the reference's tests write it
+    (pipeline.pipeline_graph.write(...)): one cluster per group, one node
+    per stage, one edge per producer-consumer pair, live-outs bold."""
+    p = build_harris(tile_sizes=(32, 128))
+    g = p.pipeline_graph
+    path = tmp_path / "harris.dot"
+    g.write(str(path))
+    text = path.read_text()
+    assert text.startswith('digraph "harris"')
+    assert text.count("subgraph") == len(p.groups) == 1
+    nodes = [l for l in text.splitlines() if "shape=box" in l]
+    assert len(nodes) == len(p.comps) == 11
+    edges = sum(len(c.parents) for c in p.comps)
+    assert text.count("->") == edges
+    assert '"harris" [shape=box, style="rounded, bold"' in text
