@@ -273,3 +273,15 @@ def test_pipeline_graph_dot(tmp_path):
     edges = sum(len(c.parents) for c in p.comps)
     assert text.count("->") == edges
     assert '"harris" [shape=box, style="rounded, bold"' in text
+
+
+def test_jacobi_steps_fuse_into_one_time_tiled_group():
+    """Four Jacobi steps (one function each) fuse into one overlapped-tile
+    group: the time loop is tiled with the space loops; the kernel
+    computes in double precision."""
+    from polymage_b200.apps.jacobi import build_jacobi2d
+    p = build_jacobi2d(N=1022, T=4)
+    assert len(p.groups) == 1 and len(p.groups[0].comps) == 4
+    src = p.generate_code().source
+    assert "double" in src and "4.0f" not in src
+    assert p.build().so_path.endswith(".so")

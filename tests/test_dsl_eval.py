@@ -109,3 +109,13 @@ def test_campipe_statement_matches_c_restatement():
     got = ev.array(camera_pipe({}))
     d = np.abs(got - OC.campipe(img, 3700.0, 50.0, 2.0).astype(np.float64))
     assert d.max() <= 1 and (d > 0).mean() <= 0.01
+
+
+def test_jacobi_restatement_matches_statement():
+    import oracle.jacobi as OJ
+    from polymage_b200.apps.jacobi import jacobi2d
+    for N, T in ((10, 1), (13, 4)):
+        V, F = OJ.make_input(N, seed=N)
+        got = Evaluator({'N': N}, {'V_': V, 'F_': F}).array(
+            jacobi2d({}, T=T))
+        assert np.abs(got - OJ.jacobi2d(V, F, T)).max() <= 1e-12
