@@ -31,3 +31,25 @@ def jacobi2d(V, F, T=4):
 def make_input(N, seed=0):
     rng = np.random.default_rng(seed)
     return rng.random((N + 2, N + 2)), rng.random((N + 2, N + 2))
+
+
+def jacobi3d(V, F, T=2):
+    """3-D variant (stencil/jacobi3D/polymage_jacobi.py:8-60): 7-point
+    Laplacian, omega = 8/9, c = omega h^2 / 6."""
+    V = np.asarray(V, np.float64)
+    F = np.asarray(F, np.float64)
+    N = V.shape[0] - 2
+    h = 1.0 / (N + 1)
+    invhh = 1.0 / (h * h)
+    c = (8.0 / 9.0) * ((h * h) / 6.0)
+    i = slice(1, N + 1)
+    lo = slice(0, N)
+    hi = slice(2, N + 2)
+    u = V
+    for _ in range(T):
+        w = np.zeros_like(u)
+        w[i, i, i] = u[i, i, i] - c * ((
+            u[i, i, i] * 6.0 - u[lo, i, i] - u[hi, i, i] - u[i, lo, i] -
+            u[i, hi, i] - u[i, i, lo] - u[i, i, hi]) * invhh - F[i, i, i])
+        u = w
+    return u

@@ -285,3 +285,5 @@ def test_jacobi_steps_fuse_into_one_time_tiled_group():
     src = p.generate_code().source
     assert "double" in src and "4.0f" not in src
     assert p.build().so_path.endswith(".so")
+    from polymage_b200.apps.jacobi import build_jacobi3d
+    assert build_jacobi3d(N=126, T=2).build().so_path.endswith(".so")

@@ -119,3 +119,13 @@ def test_jacobi_restatement_matches_statement():
         got = Evaluator({'N': N}, {'V_': V, 'F_': F}).array(
             jacobi2d({}, T=T))
         assert np.abs(got - OJ.jacobi2d(V, F, T)).max() <= 1e-12
+
+
+def test_jacobi3d_restatement_matches_statement():
+    import oracle.jacobi as OJ
+    from polymage_b200.apps.jacobi import jacobi3d
+    N, T = 6, 2
+    rng = np.random.default_rng(1)
+    V, F = rng.random((N + 2,) * 3), rng.random((N + 2,) * 3)
+    got = Evaluator({'N': N}, {'V_': V, 'F_': F}).array(jacobi3d({}, T=T))
+    assert np.abs(got - OJ.jacobi3d(V, F, T)).max() <= 1e-12
