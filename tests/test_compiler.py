@@ -287,3 +287,15 @@ def test_jacobi_steps_fuse_into_one_time_tiled_group():
     assert p.build().so_path.endswith(".so")
     from polymage_b200.apps.jacobi import build_jacobi3d
     assert build_jacobi3d(N=126, T=2).build().so_path.endswith(".so")
+
+
+def test_v_cycle_plans_and_compiles():
+    """The multigrid V-cycle (3 levels: smoothing, defect, restriction,
+    interpolation with correction) fuses across levels and compiles; its
+    entry point keeps the reference's name."""
+    from polymage_b200.apps.multigrid import build_v_cycle
+    p = build_v_cycle(n=63, L=2)
+    assert 2 <= len(p.groups) <= 8
+    cp = p.build()
+    assert cp.so_path.endswith(".so")
+    assert "pipeline_Vcycle(" in p.generate_code().source

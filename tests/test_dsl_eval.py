@@ -129,3 +129,12 @@ def test_jacobi3d_restatement_matches_statement():
     V, F = rng.random((N + 2,) * 3), rng.random((N + 2,) * 3)
     got = Evaluator({'N': N}, {'V_': V, 'F_': F}).array(jacobi3d({}, T=T))
     assert np.abs(got - OJ.jacobi3d(V, F, T)).max() <= 1e-12
+
+
+def test_v_cycle_restatement_matches_statement():
+    import oracle.multigrid as OM
+    from polymage_b200.apps.multigrid import v_cycle
+    for n, L in ((3, 2), (4, 1), (2, 3)):
+        V, F = OM.make_input(n, L, seed=n)
+        got = Evaluator({'n': n}, {'V_': V, 'F_': F}).array(v_cycle({}, L=L))
+        assert np.abs(got - OM.v_cycle(V, F, n, L)).max() <= 1e-12
