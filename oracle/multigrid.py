@@ -82,8 +82,10 @@ def _interpolate(E, corr, N):
     return W
 
 
-def v_cycle(V, F, n, L=2, nu1=1, nu2=1, nuc=1):
-    """V, F: float64 [N_L+2]^2 with N_L = 2^L (n+1) - 1."""
+def v_cycle(V, F, n, L=2, nu1=1, nu2=1, nuc=1, gamma=1):
+    """V, F: float64 [N_L+2]^2 with N_L = 2^L (n+1) - 1; ``gamma`` 2 is
+    the W-cycle (polymage_wcycle.py:80-84: the coarse cycle twice, the
+    second from the first's result)."""
     N = [n]
     for _ in range(L):
         N.append(2 * N[-1] + 1)
@@ -99,7 +101,9 @@ def v_cycle(V, F, n, L=2, nu1=1, nu2=1, nuc=1):
             u = _smooth(u, f, N[l], l == L)
         r = f if u is None else _defect(u, f, N[l])
         r2 = _restrict(r, N[l - 1])
-        e = cycle(None, r2, l - 1)
+        e = None
+        for _ in range(gamma):
+            e = cycle(e, r2, l - 1)
         ec = u if e is None else _interpolate(e, u, N[l])
         for _ in range(nu2):
             ec = _smooth(ec, f, N[l], l == L)

@@ -1,6 +1,7 @@
-"""Multigrid V-cycle for the 2-D Poisson problem, as specified by the
-reference's multigrid app (sandbox/apps/python/multigrid/jacobi2D:
-polymage_vcycle.py:8-140, polymage_smoother.py, polymage_defect.py,
+"""Multigrid V- and W-cycles for the 2-D Poisson problem, as specified by
+the reference's multigrid app (sandbox/apps/python/multigrid/jacobi2D:
+polymage_vcycle.py:8-140, polymage_wcycle.py, polymage_smoother.py,
+polymage_defect.py,
 polymage_restrict.py, polymage_interpolate.py, polymage_common.py:16-75;
 defaults in arg_parser.py: n = 255, L = 2, nu1 = nuc = nu2 = 1).
 
@@ -31,7 +32,10 @@ from ..expr_ast import Value
 from ..compiler import buildPipeline
 
 
-def v_cycle(pipe_data=None, L=2, nu1=1, nu2=1, nuc=1, name="Vcycle"):
+def v_cycle(pipe_data=None, L=2, nu1=1, nu2=1, nuc=1, name="Vcycle",
+            gamma=1):
+    """``gamma`` coarse-grid visits per level: 1 is the V-cycle, 2 the
+    W-cycle (polymage_wcycle.py, pipeline name ``Wcycle``)."""
     assert nu1 + nu2 + nuc > 0
     n = Parameter(Int, "n")
     y = Variable(Int, "y")
@@ -115,29 +119,39 @@ def v_cycle(pipe_data=None, L=2, nu1=1, nu2=1, nuc=1, name="Vcycle"):
             ghosts(l, cv)
         return W
 
+    visits = dict((l, 0) for l in range(L + 1))
+
     def cycle(v, f, l):
+        visits[l] += 1
+        tag = "__%d" % visits[l] if gamma > 1 else ""
         if l == 0:
             if nuc == 0:
                 return v
             u = v
             for t in range(nuc):
                 fname = name if (l == L and t == nuc - 1) else \
-                    "T%d_coarse" % t
+                    "T%d_coarse%s" % (t, tag)
                 u = smooth(u, f, l, fname)
             return u
         u = v
         for t in range(nu1):
-            u = smooth(u, f, l, "T%d_pre_L%d" % (t, l))
-        r = defect(u, f, l, "defect_L%d" % l)
-        r2 = restrict(r, l, "restrict_L%d" % (l - 1))
-        e = cycle(None, r2, l - 1)
-        fname = name if (l == L and nu2 <= 0) else "interp_correct_L%d" % l
+            u = smooth(u, f, l, "T%d_pre_L%d%s" % (t, l, tag))
+        r = defect(u, f, l, "defect_L%d%s" % (l, tag))
+        r2 = restrict(r, l, "restrict_L%d%s" % (l - 1, tag))
+        # gamma coarse-grid visits: the V-cycle one, the W-cycle two, the
+        # second starting from the first one's result
+        # (polymage_wcycle.py:80-84)
+        e = None
+        for _ in range(gamma):
+            e = cycle(e, r2, l - 1)
+        fname = name if (l == L and nu2 <= 0) else \
+            "interp_correct_L%d%s" % (l, tag)
         ec = interpolate(e, u, l, fname)
         if nu2 <= 0:
             return ec
         for t in range(nu2):
             fname = name if (l == L and t == nu2 - 1) else \
-                "T%d_post_L%d" % (t, l)
+                "T%d_post_L%d%s" % (t, l, tag)
             ec = smooth(ec, f, l, fname)
         return ec
 
@@ -147,9 +161,10 @@ def v_cycle(pipe_data=None, L=2, nu1=1, nu2=1, nuc=1, name="Vcycle"):
 
 
 def build_v_cycle(n=255, L=2, nu1=1, nu2=1, nuc=1, tile_sizes=(16, 64),
-                  group_size=6, options=(), name="Vcycle"):
+                  group_size=6, options=(), name="Vcycle", gamma=1):
     data = {}
-    out = v_cycle(data, L=L, nu1=nu1, nu2=nu2, nuc=nuc, name=name)
+    out = v_cycle(data, L=L, nu1=nu1, nu2=nu2, nuc=nuc, name=name,
+                  gamma=gamma)
     p = data['n']
     return buildPipeline([out], param_estimates=[(p, n)],
                          param_constraints=[Condition(p, "==", n)],

@@ -299,3 +299,5 @@ def test_v_cycle_plans_and_compiles():
     cp = p.build()
     assert cp.so_path.endswith(".so")
     assert "pipeline_Vcycle(" in p.generate_code().source
+    w = build_v_cycle(n=63, L=2, gamma=2, name="Wcycle")
+    assert w.build().so_path.endswith(".so")

@@ -134,7 +134,8 @@ def test_jacobi3d_restatement_matches_statement():
 def test_v_cycle_restatement_matches_statement():
     import oracle.multigrid as OM
     from polymage_b200.apps.multigrid import v_cycle
-    for n, L in ((3, 2), (4, 1), (2, 3)):
+    for n, L, g in ((3, 2, 1), (4, 1, 1), (2, 3, 1), (3, 2, 2), (2, 3, 2)):
         V, F = OM.make_input(n, L, seed=n)
-        got = Evaluator({'n': n}, {'V_': V, 'F_': F}).array(v_cycle({}, L=L))
-        assert np.abs(got - OM.v_cycle(V, F, n, L)).max() <= 1e-12
+        got = Evaluator({'n': n}, {'V_': V, 'F_': F}).array(
+            v_cycle({}, L=L, gamma=g, name="Wcycle" if g == 2 else "Vcycle"))
+        assert np.abs(got - OM.v_cycle(V, F, n, L, gamma=g)).max() <= 1e-12
