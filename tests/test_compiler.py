@@ -301,3 +301,6 @@ def test_v_cycle_plans_and_compiles():
     assert "pipeline_Vcycle(" in p.generate_code().source
     w = build_v_cycle(n=63, L=2, gamma=2, name="Wcycle")
     assert w.build().so_path.endswith(".so")
+    d3 = build_v_cycle(n=31, L=2, dims=3, tile_sizes=(4, 8, 32),
+                       name="Vcycle3d")
+    assert d3.build().so_path.endswith(".so")

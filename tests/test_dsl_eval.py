@@ -139,3 +139,13 @@ def test_v_cycle_restatement_matches_statement():
         got = Evaluator({'n': n}, {'V_': V, 'F_': F}).array(
             v_cycle({}, L=L, gamma=g, name="Wcycle" if g == 2 else "Vcycle"))
         assert np.abs(got - OM.v_cycle(V, F, n, L, gamma=g)).max() <= 1e-12
+
+
+def test_v_cycle3d_restatement_matches_statement():
+    import oracle.multigrid as OM
+    from polymage_b200.apps.multigrid import v_cycle
+    for n, L, g in ((1, 2, 1), (2, 1, 1), (1, 2, 2)):
+        V, F = OM.make_input3d(n, L, seed=n)
+        got = Evaluator({'n': n}, {'V_': V, 'F_': F}).array(
+            v_cycle({}, L=L, gamma=g, dims=3))
+        assert np.abs(got - OM.v_cycle3d(V, F, n, L, gamma=g)).max() <= 1e-12
