@@ -304,3 +304,13 @@ def test_v_cycle_plans_and_compiles():
     d3 = build_v_cycle(n=31, L=2, dims=3, tile_sizes=(4, 8, 32),
                        name="Vcycle3d")
     assert d3.build().so_path.endswith(".so")
+
+
+def test_nas_mg_plans_and_compiles():
+    """NAS MG class S: two live-outs (MG_U, MG_R), restrictions down to
+    level 1 then the levels back up fused pairwise; compiles."""
+    from polymage_b200.apps.nas_mg import build_mg3p
+    p = build_mg3p('S')
+    names = [c.func.name for g in p.groups for c in g.comps]
+    assert "MG_U" in names and "MG_R" in names
+    assert p.build().so_path.endswith(".so")

@@ -149,3 +149,16 @@ def test_v_cycle3d_restatement_matches_statement():
         got = Evaluator({'n': n}, {'V_': V, 'F_': F}).array(
             v_cycle({}, L=L, gamma=g, dims=3))
         assert np.abs(got - OM.v_cycle3d(V, F, n, L, gamma=g)).max() <= 1e-12
+
+
+def test_nas_mg_restatement_matches_statement():
+    """Both outputs of the NAS MG V-cycle (MG_U, MG_R)."""
+    import oracle.nas_mg as ON
+    from polymage_b200.apps.nas_mg import mg3p
+    for n in (8, 16):
+        U, V, R = ON.make_input(n, seed=n)
+        u, r = mg3p({}, lt=n.bit_length() - 1, prob_class='S')
+        ev = Evaluator({'n': n}, {'U': U, 'V': V, 'R': R})
+        ou, orr = ON.mg3p(U, V, R, 'S')
+        assert np.abs(ev.array(u) - ou).max() <= 1e-12
+        assert np.abs(ev.array(r) - orr).max() <= 1e-12
