@@ -314,3 +314,48 @@ def test_nas_mg_plans_and_compiles():
     names = [c.func.name for g in p.groups for c in g.comps]
     assert "MG_U" in names and "MG_R" in names
     assert p.build().so_path.endswith(".so")
+
+
+def _next_app(name):
+    if name == "interpolate":
+        from polymage_b200.apps.interpolate import build_interpolate
+        return build_interpolate(rows=128, cols=160), {'R': 128, 'C': 160}
+    if name == "jacobi2d":
+        from polymage_b200.apps.jacobi import build_jacobi2d
+        return build_jacobi2d(N=200, T=4), {'N': 200}
+    if name == "vcycle":
+        from polymage_b200.apps.multigrid import build_v_cycle
+        return build_v_cycle(n=15, L=2), {'n': 15}
+    if name == "wcycle3d":
+        from polymage_b200.apps.multigrid import build_v_cycle
+        return (build_v_cycle(n=7, L=2, dims=3, gamma=2, name="Wcycle3d",
+                              tile_sizes=(4, 8, 32)), {'n': 7})
+    from polymage_b200.apps.nas_mg import build_mg3p
+    return build_mg3p('S'), {'n': 32}
+
+
+@pytest.mark.parametrize("name", ["interpolate", "jacobi2d", "vcycle",
+                                  "wcycle3d", "nas_mg"])
+def test_static_extents_cover_every_tile_next_apps(name):
+    """The same tile-by-tile check for the apps not yet run on a GPU."""
+    p, sizes = _next_app(name)
+    env = p.int_env()
+    for k in list(env):
+        if k.name in sizes:
+            env[k] = sizes[k.name]
+    checked = 0
+    for g in p.groups:
+        plan = g.plan
+        if getattr(plan, 'kind', None) != 'stencil':
+            continue
+        for box in _tile_boxes(plan, env):
+            regs = infer_regions(plan, box, env)
+            for n in plan.nodes:
+                if not n.in_smem:
+                    continue
+                lo, hi = regs[n.func]
+                for d in range(n.ndims):
+                    ext = int(hi[d]) - int(lo[d]) + 1
+                    assert ext <= n.ext[d], (n.name, d, ext, n.ext[d], box)
+            checked += 1
+    assert checked > 0
