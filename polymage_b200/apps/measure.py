@@ -151,6 +151,37 @@ def measure(app, steps=50, warmup=5, device=None, graph=True, warm=False):
                    "256 MB written before each timed run")}
 
 
+def measure_host(app, steps=10, warmup=2):
+    """End to end through the reference's C ABI (``pipeline_<name>`` on
+    pinned host buffers: copies to and from the device inside the call),
+    host wall clock over ``steps`` calls, as bench.py's ``e2e``."""
+    import time
+    import torch
+    cp = catalog.build(app)
+    prm, host_in, out_spec, pixels, desc = workload(app)
+    ins = {}
+    for k, v in host_in.items():
+        t = torch.from_numpy(v).pin_memory()
+        ins[k] = t.numpy()
+    outs = {}
+    for k, (shape, dt) in out_spec.items():
+        t = torch.zeros(shape, dtype=torch.from_numpy(
+            np.zeros(1, dt)).dtype).pin_memory()
+        outs[k] = t.numpy()
+    for _ in range(warmup):
+        cp.run_host(prm, ins, outs)
+    s0 = time.perf_counter()
+    for _ in range(steps):
+        cp.run_host(prm, ins, outs)
+    sec = (time.perf_counter() - s0) / steps
+    h2d = sum(v.nbytes for v in ins.values())
+    d2h = sum(v.nbytes for v in outs.values())
+    return {"app": app, "workload": desc, "api": "pipeline_%s (host "
+            "buffers, pinned)" % cp.name, "ms": sec * 1e3,
+            "mpix_s": pixels / sec / 1e6, "h2d_bytes": int(h2d),
+            "d2h_bytes": int(d2h)}
+
+
 def measure_bilateral_batch(n=64, steps=10, warmup=3, graph=True,
                             device=None, seed=1):
     """The batched bilateral-grid workload: ``n`` images whose sides are
@@ -235,6 +266,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--warm", action="store_true",
                     help="no L2 flush between runs (single-image pipelines)")
+    ap.add_argument("--host", action="store_true",
+                    help="end to end through the host-buffer C ABI")
     args = ap.parse_args()
     for app in args.app or APPS + ("bilateral_batch64", "stream1024"):
         if app == "stream1024":
@@ -242,6 +275,8 @@ def main():
         elif app == "bilateral_batch64":
             print(json.dumps(measure_bilateral_batch(
                 64, steps=min(args.steps, 10), warmup=args.warmup)))
+        elif args.host:
+            print(json.dumps(measure_host(app, min(args.steps, 20))))
         else:
             print(json.dumps(measure(app, args.steps, args.warmup,
                                      warm=args.warm)))
