@@ -64,7 +64,7 @@ from .expr_ast import (Value, AbstractBinaryOpNode, AbstractUnaryOpNode,
 from .expression import substitute_vars, getType, affine_form
 from .bounds import part_boxes
 from .pipe import body_parts
-from .tiling import IndexFn, is_data_dependent
+from .tiling import is_data_dependent
 from .evaluate import monotone_dir, is_min_max
 
 _INT_T = (C.Int, C.UInt, C.Short, C.UShort, C.Char, C.UChar, C.Long,

@@ -12,8 +12,7 @@ from fractions import Fraction
 
 import numpy as np
 
-from .expr_ast import (Value, AbstractBinaryOpNode, AbstractUnaryOpNode,
-                       InbuiltFunction)
+from .expr_ast import Value, AbstractBinaryOpNode, AbstractUnaryOpNode
 from . import constructs as C
 
 

@@ -21,7 +21,7 @@ import logging
 from .expr_ast import Value
 from . import constructs as C
 from .expression import rebuild, rebuild_cond
-from .evaluate import eval_int, EvalError
+from .evaluate import eval_int
 
 LOG = logging.getLogger("polymage_b200.pipe")
 
