@@ -79,3 +79,31 @@ def test_checker_catches_a_missing_wait():
     sof, waits, _ = streams.schedule(rw, 4)
     assert streams.check(rw, sof, waits) and waits[2]
     assert not streams.check(rw, sof, [[], [], []])
+
+
+@pytest.mark.parametrize("name", ["laplacian", "pyramid8", "vcycle",
+                                  "wcycle", "nas_mg", "interpolate"])
+def test_schedules_of_larger_pipelines_keep_every_order(name):
+    """Deeper DAGs with workspace slots reused across many groups."""
+    if name in ("laplacian", "pyramid8"):
+        b, kw = catalog._BUILDERS[name]
+        p = b(**kw)
+    elif name == "vcycle":
+        from polymage_b200.apps.multigrid import build_v_cycle
+        p = build_v_cycle(n=63, L=3)
+    elif name == "wcycle":
+        from polymage_b200.apps.multigrid import build_v_cycle
+        p = build_v_cycle(n=63, L=3, gamma=2, name="Wcycle")
+    elif name == "nas_mg":
+        from polymage_b200.apps.nas_mg import build_mg3p
+        p = build_mg3p('S')
+    else:
+        from polymage_b200.apps.interpolate import build_interpolate
+        p = build_interpolate(rows=512, cols=512)
+    p.generate_code()
+    pg = PipelineGen(p)
+    pg.slot_of = getattr(p, '_storage_assign', {})
+    rw = [pg.group_rw(g) for g in p.groups]
+    for nst in (2, 3, 4):
+        sof, waits, _ = streams.schedule(rw, nst)
+        assert streams.check(rw, sof, waits)
