@@ -1943,8 +1943,13 @@ class StencilGen(object):
             al = max(1, 16 // es)
             ext[-1] = n.pad_inner
             nd = n.ndims
-            w("const int so_%s_%d = (r_%s_lo%d - d_%s_lo%d) & ~%d;" % (
-                nm, nd - 1, nm, nd - 1, fnm, nd - 1, al - 1))
+            if getattr(n, 'tight', False):
+                # the whole innermost dimension, narrower than one 16-byte
+                # chunk: the rounded-down origin offset is always 0
+                w("const int so_%s_%d = 0;" % (nm, nd - 1))
+            else:
+                w("const int so_%s_%d = (r_%s_lo%d - d_%s_lo%d) & ~%d;" % (
+                    nm, nd - 1, nm, nd - 1, fnm, nd - 1, al - 1))
             org = ["r_%s_lo%d" % (nm, d) for d in range(nd - 1)] + \
                 ["(d_%s_lo%d + so_%s_%d)" % (fnm, nd - 1, nm, nd - 1)]
         else:

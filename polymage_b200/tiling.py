@@ -537,7 +537,7 @@ def plan_stencil(pipeline, comps):
 
     _static_extents(plan, env)
     _alignment(plan, env)
-    _layout_smem(plan)
+    _layout_smem(plan, tight=('tight_stage' in pipeline.options), env=env)
     if plan.smem_bytes > int(_option(pipeline, 'smem_budget', SMEM_BUDGET)):
         raise PlanError("shared memory %d B exceeds budget" %
                         plan.smem_bytes)
@@ -847,7 +847,14 @@ def _alignment(plan, env):
                     raise PlanError("inconsistent scaling of %s" % n.name)
 
 
-def _layout_smem(plan):
+def _layout_smem(plan, tight=False, env=None):
+    """Shared-memory buffers, placed first-fit by lifetime.  A staged
+    input's rows carry the slack a TMA box needs when its origin is
+    rounded down to 16 bytes; with ``tight`` (option 'tight_stage') an
+    input whose innermost dimension is staged whole and is narrower than
+    16 bytes (the channels of an interleaved uint8 image), which no tensor
+    map can describe, gets rows of exactly that width: its origin offset
+    is then always 0 and the cooperative loads cover only used bytes."""
     bufs = []
     for n in plan.nodes:
         if not n.in_smem:
@@ -855,9 +862,16 @@ def _layout_smem(plan):
             continue
         es = n.func.typ.size()
         ext = list(n.ext)
+        n.tight = False
         if n.role == 'stage':
             al = max(1, 16 // es)
-            w = ((ext[-1] + al - 1 + al - 1) // al) * al
+            whole = env is not None and _const_extent(
+                n.func.domain[-1], env) == ext[-1]
+            if tight and whole and ext[-1] < al:
+                w = ext[-1]
+                n.tight = True
+            else:
+                w = ((ext[-1] + al - 1 + al - 1) // al) * al
             n.pad_inner = w
             ext[-1] = w
         elif es == 4 and ext[-1] % 4 and ext[-1] > 4:

@@ -359,3 +359,26 @@ def test_static_extents_cover_every_tile_next_apps(name):
                     assert ext <= n.ext[d], (n.name, d, ext, n.ext[d], box)
             checked += 1
     assert checked > 0
+
+
+def test_tight_staging_of_interleaved_channels():
+    """Option 'tight_stage': the local Laplacian's uint8 [x][y][3] frame is
+    staged with rows of 3 bytes (no TMA slack): the cooperative load loop
+    covers 32 x 64 x 3 bytes instead of 32 x 64 x 32, the origin offset is
+    0, and the default layout is unchanged."""
+    import re
+    from polymage_b200.apps.local_laplacian import build_laplacian
+    loops = {}
+    for opts in (('rblock=8',), ('rblock=8', 'tight_stage')):
+        p = build_laplacian(rows=270, cols=480, options=opts)
+        src = p.generate_code().source
+        seg = src[src.index('pm_laplacian_g0(const'):]
+        seg = seg[:seg.index('// stage')]
+        loops[len(opts)] = int(re.findall(
+            r'for \(int i = threadIdx.x; i < (\d+);', seg)[0])
+        if len(opts) == 2:
+            assert 'so_img_colour_2 = 0;' in seg
+            assert p.build().so_path.endswith(".so")
+        else:
+            assert '& ~15;' in seg
+    assert loops[1] == 32 * 64 * 32 and loops[2] == 32 * 64 * 3
