@@ -274,8 +274,24 @@ class ExprCtx(object):
             b = self.expr(e.false_expression, bind)
             return "(%s ? %s : %s)" % (c, a, b)
         if isinstance(e, InbuiltFunction):
-            args = ", ".join(self.expr(a, bind) for a in e.arguments)
-            return "%s(%s)" % (self._fname(e), args)
+            args = []
+            for a in e.arguments:
+                t = self.expr(a, bind)
+                # C promotes an integer argument of a math function to
+                # double (to float for the f-suffixed ones); CUDA has no
+                # device overload taking an integer, so the conversion is
+                # written out
+                if self.mode == 'device' and not isinstance(e, C.Abs):
+                    try:
+                        it = getType(a) in _INT_T
+                    except Exception:
+                        it = False
+                    if it:
+                        t = "((%s)(%s))" % (
+                            "float" if isinstance(e, (C.Powf, C.Sqrtf))
+                            else "double", t)
+                args.append(t)
+            return "%s(%s)" % (self._fname(e), ", ".join(args))
         raise CodegenError("cannot print %r" % (e,))
 
     def _fname(self, e):
@@ -456,6 +472,47 @@ def _has_clamp(e):
         if hasattr(n, 'children'):
             stack.extend(n.children())
     return False
+
+
+def _fixed_cells(f, cond, red):
+    """{cell coordinate: constant} that a Reduction part's condition fixes:
+    conjuncts ``v == k`` where ``v`` is the part's target argument at that
+    coordinate (a reduction variable used as the cell index) or the
+    function variable of that coordinate (which stands for the target
+    cell's index)."""
+    out = {}
+    if cond is None:
+        return out
+    pos = {}
+    for d, (fv, ta) in enumerate(zip(f.variables, red.accumulate_ref.arguments)):
+        pos.setdefault(id(fv), d)
+        if isinstance(ta, C.Variable):
+            pos.setdefault(id(ta), d)
+    stack = [cond]
+    while stack:
+        c = stack.pop()
+        if c.conditional == '&&':
+            stack.extend([c.lhs, c.rhs])
+        elif c.conditional == '==':
+            for v, k in ((c.lhs, c.rhs), (c.rhs, c.lhs)):
+                k = Value.numericToValue(k)
+                if isinstance(v, C.Variable) and id(v) in pos and \
+                        isinstance(k, Value) and isinstance(k.value, int):
+                    out[pos[id(v)]] = int(k.value)
+    return out
+
+
+def _disjoint_parts(f, parts):
+    """Whether every two parts of a Reduction update disjoint cells: each
+    fixes some cell coordinate to a constant the other fixes to a
+    different value (the per-channel operators of a histogram)."""
+    fixed = [_fixed_cells(f, cond, red) for cond, _, red in parts]
+    for i in range(len(parts)):
+        for j in range(i + 1, len(parts)):
+            if not any(k in fixed[j] and fixed[j][k] != v
+                       for k, v in fixed[i].items()):
+                return False
+    return True
 
 
 def _subst(a, bind):
@@ -2760,10 +2817,16 @@ class ReductionGen(object):
                         reads.append(r.objectRef)
         self.reads = reads
         ops = set(red.op_type for _, _, red in parts)
-        if len(ops) != 1:
-            raise CodegenError("mixed reduction operators in %s" % f.name)
-        op = ops.pop()
-        self.op = op
+        if len(ops) != 1 and not _disjoint_parts(f, parts):
+            raise CodegenError("%s: reduction parts with different "
+                               "operators may update the same cell" %
+                               f.name)
+        # one operator per part; with several, the parts update disjoint
+        # cells (a condition fixing a non-reduced variable to different
+        # constants) and accumulate straight into the output
+        self.part_ops = [red.op_type for _, _, red in parts]
+        self.op = parts[0][2].op_type
+        self.mixed = len(ops) != 1
         pg.meta['groups'].append({
             'kernel': k, 'kind': 'reduction', 'threads': plan.threads,
             'smem': plan.smem_bytes, 'tile': plan.tile,
@@ -2841,7 +2904,7 @@ class ReductionGen(object):
             w("const %s* __restrict__ b_%s = D.b_%s;" % (ctype(x.typ),
                                                          pg.fn(x), pg.fn(x)))
         w("%s* __restrict__ out = D.b_%s;" % (T, fnm))
-        priv = plan.privatize
+        priv = plan.privatize and not self.mixed
         if priv:
             # privatized box: union of target footprints of this tile
             for d in range(nd):
@@ -2915,7 +2978,8 @@ class ReductionGen(object):
             else:
                 gidx = " + ".join("(long long)(%s - d_%s_lo%d) * s_%s_%d" % (
                     cn[d], fnm, d, fnm, d) for d in range(nd))
-                w("%s(&out[%s], (%s)(%s));" % (self.atomic(), gidx, T, val))
+                w("%s(&out[%s], (%s)(%s));" % (
+                    self.atomic(self.part_ops[pi]), gidx, T, val))
             w.close()
             if not shared:
                 w.close()
@@ -2941,9 +3005,10 @@ class ReductionGen(object):
         w("")
         self.gen_launcher()
 
-    def atomic(self):
+    def atomic(self, op=None):
         return {C.Op.Sum: 'pm_atomic_add', C.Op.Mul: 'pm_atomic_mul',
-                C.Op.Min: 'pm_atomic_min', C.Op.Max: 'pm_atomic_max'}[self.op]
+                C.Op.Min: 'pm_atomic_min',
+                C.Op.Max: 'pm_atomic_max'}[self.op if op is None else op]
 
     def identity(self):
         T = self.f.typ

@@ -137,7 +137,13 @@ class Evaluator(object):
             return int(v) if e.typ in _INTS else float(v)
         for cls, fn in _BUILTINS.items():
             if isinstance(e, cls):
-                return fn(*[self.expr(a, env) for a in e.arguments])
+                args = [self.expr(a, env) for a in e.arguments]
+                try:
+                    return fn(*args)
+                except ValueError:          # C: a domain error is NaN
+                    return float('nan')
+                except OverflowError:
+                    return float('inf')
         raise NotImplementedError(type(e).__name__)
 
     def array(self, f, params_shape=None):
