@@ -120,8 +120,12 @@ def auto_group(pipeline):
 
 def manual_group(pipeline, grouping):
     """User-specified grouping: a list of lists of Functions (the original
-    objects passed to buildPipeline).  Functions not listed stay alone."""
+    objects passed to buildPipeline).  Functions not listed stay alone, and
+    so does a Function given directly as an entry (the reference's tests
+    also pass a flat list: sandbox/tests/test_stencil.py:58)."""
     for funcs in grouping:
+        if not isinstance(funcs, (list, tuple)):
+            funcs = [funcs]
         comps = []
         for f in funcs:
             clone = pipeline._clone_map.get(f, f)

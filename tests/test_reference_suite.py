@@ -296,3 +296,43 @@ def test_alignment_permuted_dimensions(case):
     p = buildPipeline([out], grouping=groups, param_estimates=est)
     assert len(p.groups) == 1
     assert len(p.generate_code().source) > 0
+
+
+def test_stencil_pipeline(tmp_path):
+    """sandbox/tests/test_stencil.py:10-60: two stages defined by Stencil
+    macros (a 3x3 and a 2x3 kernel), grouping given as a flat list."""
+    R = Parameter(Int, "R")
+    C = Parameter(Int, "C")
+    x = Variable(Int, "x")
+    y = Variable(Int, "y")
+    xrow = Interval(Int, 1, R)
+    xcol = Interval(Int, 1, C)
+    bounds = (Condition(x, '>=', 2) & Condition(x, '<=', R - 2) &
+              Condition(y, '>=', 2) & Condition(y, '<=', C - 2))
+    img = Image(Float, "input", [R + 2, C + 2])
+    k1 = [[1, 0, 0], [0, 2, 0], [0, 0, 1]]
+    f1 = Function(([x, y], [xrow, xcol]), Float, "f1")
+    f1.defn = [Case(bounds, Stencil(img, [x, y], k1))]
+    k2 = [[-1, 2, -3.8], [0, -1, 0]]
+    f2 = Function(([x, y], [xrow, xcol]), Float, "f2")
+    f2.defn = [Case(bounds, Stencil(f1, [x, y], k2))]
+    p = buildPipeline([f2], grouping=[f1, f2],
+                      param_estimates=[(R, 1024), (C, 1024)],
+                      pipe_name="stencil")
+    _graph_ok(p, tmp_path, "stencil")
+    assert "pipeline_stencil(" in p.generate_code().source
+    # f2 = -f1(x, y-1) + 2 f1(x, y) - 3.8 f1(x, y+1) - f1(x+1, y) with
+    # f1 = img(x-1, y-1) + 2 img(x, y) + img(x+1, y+1) on its Case box
+    # [2, R-2] x [2, C-2] and 0 elsewhere (never computed there)
+    v = np.random.default_rng(3).random((10, 11))
+    got = Evaluator({'R': 8, 'C': 9}, {'input': v}).array(f2)
+
+    def f1v(i, j):
+        if not (2 <= i <= 6 and 2 <= j <= 7):
+            return 0.0
+        return v[i - 1, j - 1] + 2 * v[i, j] + v[i + 1, j + 1]
+    for i in range(2, 7):
+        for j in range(2, 8):
+            ref = (-f1v(i, j - 1) + 2 * f1v(i, j) - 3.8 * f1v(i, j + 1) -
+                   f1v(i + 1, j))
+            assert abs(got[i - 1, j - 1] - ref) < 1e-12
