@@ -3,8 +3,12 @@
 
 The reference inlines a directive's function when every use reads values
 produced by one predicate-free piece of its definition.  This backend
-inlines functions whose definition is a single expression (no ``Case``),
-which is always safe, and keeps the others with a warning.  Independently
+inlines functions whose definition is a single expression, and those
+defined by a single ``Case(cond, e)``, which become ``Select(cond, e, 0)``
+at each use: the value of a point the Case does not cover is 0, the
+convention for uncomputed points, so the substitution is exact whether or
+not the reads stay inside the Case.  Piecewise definitions are kept, with
+a warning.  Independently
 of directives, the CUDA code generator computes cheap pointwise stages in
 registers at their use points (tiling.py), which is where most of the
 reference's explicit inlining benefit comes from on a GPU.
@@ -13,6 +17,7 @@ reference's explicit inlining benefit comes from on a GPU.
 import logging
 
 from . import constructs as C
+from .expr_ast import Value
 from .expression import rebuild, rebuild_cond, substitute_vars
 
 LOG = logging.getLogger("polymage_b200.inline")
@@ -21,6 +26,12 @@ LOG = logging.getLogger("polymage_b200.inline")
 def _single_expression(func):
     d = func.defn
     return len(d) == 1 and not isinstance(d[0], (C.Case, C.Reduce))
+
+
+def _single_case(func):
+    d = func.defn
+    return len(d) == 1 and isinstance(d[0], C.Case) and \
+        not isinstance(d[0].expression, C.Reduce)
 
 
 def inline_pass(pipeline):
@@ -36,11 +47,16 @@ def inline_pass(pipeline):
             LOG.warning("cannot inline %s (output, reduction or const)",
                         clone.name)
             continue
-        if not _single_expression(clone):
+        if _single_expression(clone):
+            body = clone.defn[0]
+        elif _single_case(clone):
+            case = clone.defn[0]
+            body = C.Select(case.condition, case.expression,
+                            Value(0, clone.typ), typeCheck=False)
+        else:
             LOG.warning("not inlining %s: piecewise definitions are kept",
                         clone.name)
             continue
-        body = clone.defn[0]
 
         def leaf(n, clone=clone, body=body):
             if isinstance(n, C.Reference) and n.objectRef is clone:

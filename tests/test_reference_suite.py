@@ -336,3 +336,63 @@ def test_stencil_pipeline(tmp_path):
             ref = (-f1v(i, j - 1) + 2 * f1v(i, j) - 3.8 * f1v(i, j + 1) -
                    f1v(i + 1, j))
             assert abs(got[i - 1, j - 1] - ref) < 1e-12
+
+
+def test_harris_with_inline_directives(tmp_path):
+    """sandbox/tests/test_harris.py:8-110: Harris with the products, det
+    and trace inlined by directive, and an explicit zero Case at (0, 0);
+    the statement reproduces the pinned Harris oracle."""
+    import oracle.harris as OH
+    R = Parameter(Int, "R")
+    C = Parameter(Int, "C")
+    x = Variable(Int, "x")
+    y = Variable(Int, "y")
+    row = Interval(Int, 0, R + 1)
+    col = Interval(Int, 0, C + 1)
+    cond = (Condition(x, '>=', 1) & Condition(x, '<=', R) &
+            Condition(y, '<=', C) & Condition(y, '>=', 1))
+    cred = (Condition(x, '>=', 2) & Condition(x, '<=', R - 1) &
+            Condition(y, '<=', C - 1) & Condition(y, '>=', 2))
+    img = Image(Float, "img", [R + 2, C + 2])
+
+    def fn(name, c, e):
+        f = Function(([x, y], [row, col]), Float, name)
+        f.defn = [Case(c, e)]
+        return f
+    Iy = fn("Iy", cond, img(x - 1, y - 1) * (-1.0 / 12) +
+            img(x - 1, y + 1) * (1.0 / 12) + img(x, y - 1) * (-2.0 / 12) +
+            img(x, y + 1) * (2.0 / 12) + img(x + 1, y - 1) * (-1.0 / 12) +
+            img(x + 1, y + 1) * (1.0 / 12))
+    Ix = fn("Ix", cond, img(x - 1, y - 1) * (-1.0 / 12) +
+            img(x + 1, y - 1) * (1.0 / 12) + img(x - 1, y) * (-2.0 / 12) +
+            img(x + 1, y) * (2.0 / 12) + img(x - 1, y + 1) * (-1.0 / 12) +
+            img(x + 1, y + 1) * (1.0 / 12))
+    Ixx = fn("Ixx", cond, Ix(x, y) * Ix(x, y))
+    Iyy = fn("Iyy", cond, Iy(x, y) * Iy(x, y))
+    Ixy = fn("Ixy", cond, Ix(x, y) * Iy(x, y))
+
+    def box3(f):
+        return sum(f(x + i, y + j) for i in (-1, 0, 1) for j in (-1, 0, 1))
+    Sxx = fn("Sxx", cred, box3(Ixx))
+    Syy = fn("Syy", cred, box3(Iyy))
+    Sxy = fn("Sxy", cred, box3(Ixy))
+    det = fn("det", cred, Sxx(x, y) * Syy(x, y) - Sxy(x, y) * Sxy(x, y))
+    trace = fn("trace", cred, Sxx(x, y) + Syy(x, y))
+    harris = fn("harris", cred, det(x, y) - 0.04 * trace(x, y) * trace(x, y))
+    harris.defn.append(Case(Condition(x, '==', 0) & Condition(y, '==', 0),
+                            0.0))
+    p = buildPipeline([harris], inline_directives=[Ixx, Iyy, Ixy, det, trace],
+                      param_estimates=[(R, 1024), (C, 1024)],
+                      pipe_name="harris_ref")
+    names = set(c.func.name for c in p.comps)
+    assert not names & {"Ixx", "Iyy", "Ixy", "det", "trace"}
+    _graph_ok(p, tmp_path, "harris")
+    assert p.build().so_path.endswith(".so")
+    im = OH.make_input(16, 20, seed=4)
+    ref = OH.harris(im)
+    # the statement, and the pipeline's copy after inlining (the inlined
+    # single-Case functions became Selects in their consumers)
+    for f in (harris, p._clone_map[harris]):
+        got = Evaluator({'R': 14, 'C': 18},
+                        {'img': im.astype(np.float64)}).array(f)
+        assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
