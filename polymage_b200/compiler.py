@@ -2,14 +2,27 @@
 
 ``buildPipeline`` keeps the reference's keyword arguments and defaults:
 ``group_size`` 5, ``tile_sizes`` [16, 16, 16], ``size_threshold`` 200*200,
-and ``optimize_storage`` implying ``flatten_scratchpad``.  Options may also
-carry CUDA-target settings as ``"name=value"`` strings or ``(name, value)``
-tuples: ``threads`` (CTA size), ``inline_budget`` (register-recompute budget
-per consumer point), ``smem_budget`` (bytes per CTA), ``tile`` (tile sizes
-overriding ``tile_sizes``), ``materialize`` (list of function names kept in
-shared memory), ``no_stage`` (never stage inputs in shared memory),
-``no_privatize`` (reductions accumulate straight into HBM),
-``no_storage_reuse``.
+and ``optimize_storage`` implying ``flatten_scratchpad``.  The reference's
+C-target options (``early_free``, ``pool_alloc``, ``multipar``) are
+accepted and have no effect.  Options may also carry CUDA-target settings
+as ``"name=value"`` strings or ``(name, value)`` tuples:
+
+* kernel shape: ``threads`` (CTA size), ``rblock=K`` (rows per thread on
+  interior tiles), ``min_blocks=N`` (resident CTAs per SM asked of ptxas),
+  ``tile`` (tile sizes overriding ``tile_sizes``), ``red_tile`` (tile of
+  a Reduction's domain);
+* fusion and storage: ``inline_budget`` (register-recompute budget per
+  consumer point), ``smem_budget`` (bytes per CTA), ``materialize`` (names
+  kept in shared memory), ``no_stage`` (never stage inputs in shared
+  memory), ``tight_stage`` (no TMA slack for narrow whole innermost
+  dimensions), ``no_privatize`` (reductions accumulate straight into
+  HBM), ``no_storage_reuse``;
+* launches: ``streams=N`` (concurrent streams for independent groups, 1
+  for the caller's stream only);
+* switches of single optimisations, for measurement and debugging:
+  ``no_inside`` (every tile on the general path), ``guarded`` (one point
+  per iteration), ``no_vec``, ``no_cblock``, ``no_static_res``,
+  ``no_fold_clamps``.
 """
 
 from .pipe import Pipeline
