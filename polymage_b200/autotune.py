@@ -126,7 +126,7 @@ def main():
     ap.add_argument('--learned', action='store_true',
                     help='online learned tuning (cost model)')
     ap.add_argument('--compare', action='store_true',
-                    help='learned tuning, then exhaustive tuning as judge')
+                    help='learned tuning, then exhaustive tuning to compare')
     ap.add_argument('--picks', type=int, default=14,
                     help='configurations the learned tuner times (one '
                          'compile round)')

@@ -9,7 +9,7 @@ the hand-written kernels of ``csrc/mlp.cu`` (forward, backward, Adam) on the
 measurements the tuner appends to its timing database, and ranks
 configurations so that only the top-k are compiled and timed
 (``learned_tune``); the exhaustive tuner stays as the fallback and as the
-judge of the ranking.
+measure of the ranking's error.
 """
 
 import ctypes
