@@ -2,9 +2,10 @@
 (sandbox/apps/python/img_proc/bilateral_grid/polymage_bilateral_grid.py:
 16-130) -- test infrastructure only.
 
-The z bin and its fraction follow the C types of the reference's generated
-code: ``img * 10`` is a float product (float * int), truncated to int
-(:57-63, :93-97); the rest is evaluated in double.  Grid points that no
+The z bin follows the C types of the reference's generated code: ``img *
+10`` is a float product (float * int), truncated to int (:57-63, :93-97),
+so every point falls into the bin the compiled code puts it in; the rest,
+the fraction ``img * 10 - bin`` included, is evaluated in double.  Grid points that no
 ``Case`` covers read as 0 (blury at z = 12 and at the last row/column
 block, which the reference leaves uninitialized); splats whose z bin falls outside the grid (inputs >=
 1.4) are dropped.
@@ -45,7 +46,7 @@ def bilateral(img):
     blurx = _blur(blurz, 1, interior)
     blury = _blur(blurx, 2, interior)
     zi = zb
-    zf = (zv32 - zi.astype(np.float32)).astype(np.float64)   # float - int
+    zf = img.astype(np.float64) * 10 - zi         # the fraction in FP64
     xf = (x % 8).astype(np.float32) / np.float32(8)
     yf = (y % 8).astype(np.float32) / np.float32(8)
     xf = xf.astype(np.float64)

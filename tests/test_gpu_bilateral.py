@@ -43,3 +43,19 @@ def test_bilateral_device_abi_repeatable(cp, cuda):
         torch.cuda.synchronize()
         cp.check()
         assert np.abs(out.cpu().numpy() - ref).max() <= 1e-5
+
+
+def test_bilateral_matches_reference_spec_fixtures(cp):
+    """Against the reference's own bilateral_grid spec evaluated in FP64
+    (tests/golden/bilateral_spec.npz), same tolerance."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden",
+                             "bilateral_spec.npz"))
+    for n in range(2):
+        img = z['img%d' % n]
+        rows, cols = img.shape
+        out = np.zeros((1, rows, cols), np.float32)
+        cp.run_host({'rows': rows, 'cols': cols}, {'input': img},
+                    {'filtered': out})
+        assert np.abs(out.astype(np.float64) - z['fp64%d' % n]).max() \
+            <= 1e-5

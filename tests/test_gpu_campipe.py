@@ -59,3 +59,22 @@ def test_campipe_too_small_refused(cp):
                      'contrast': 50.0, 'gamma': 2.0},
                     {'img': img, 'matrix_3200': OC.MATRIX_3200,
                      'matrix_7000': OC.MATRIX_7000}, {'process': out})
+
+
+def test_campipe_matches_reference_spec_fixtures(cp):
+    """Byte for byte against the reference's own camera_pipe spec
+    evaluated with C semantics (tests/golden/campipe_spec.npz), at two
+    parameter sets and an odd image width."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden",
+                             "campipe_spec.npz"))
+    for n in range(2):
+        img = z['img%d' % n]
+        R, C = img.shape
+        kelvin, contrast, gamma = (float(v) for v in z['params%d' % n])
+        out = np.zeros((3, R - 48, C - 64), np.uint8)
+        cp.run_host({'C': C, 'R': R, 'colour_temp': kelvin,
+                     'contrast': contrast, 'gamma': gamma},
+                    {'img': img, 'matrix_3200': OC.MATRIX_3200,
+                     'matrix_7000': OC.MATRIX_7000}, {'process': out})
+        assert np.array_equal(out, z['out%d' % n])

@@ -26,3 +26,19 @@ def test_pyramid_host_abi(cp, R, C):
     ref = OP.pyramid_blend(img1, img2, mask)
     err = np.abs(out.astype(np.float64) - ref).max()
     assert err <= 2e-5, err
+
+
+def test_pyramid_matches_reference_spec_fixtures(cp):
+    """Against the reference's own pyramid_blending spec evaluated in FP64
+    (tests/golden/pyramid_spec.npz), same tolerance."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden",
+                             "pyramid_spec.npz"))
+    for n in range(2):
+        R, C = (int(v) for v in z['shape%d' % n])
+        img1, img2, mask = OP.make_inputs(R, C, seed=R)
+        ref = z['fp64%d' % n]
+        out = np.zeros(ref.shape, np.float32)
+        cp.run_host({'R': R, 'C': C}, {'img1': img1, 'img2': img2,
+                                       'mask': mask}, {'blend': out})
+        assert np.abs(out.astype(np.float64) - ref).max() <= 2e-5

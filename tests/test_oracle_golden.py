@@ -1,5 +1,9 @@
-"""The oracle's restatements pinned to the reference's own generated C++
-(golden fixtures in tests/golden, made by tests/golden/make_golden.py)."""
+"""The oracle's restatements pinned to the reference: to its own generated
+C++ (Harris, unsharp, local Laplacian; fixtures made by
+tests/golden/make_golden.py) and, for the pipelines it ships no generated
+code for (camera pipe, bilateral grid, pyramid blending), to its own DSL
+specs evaluated point by point (fixtures made by
+tests/golden/make_spec_golden.py)."""
 
 import os
 
@@ -69,3 +73,52 @@ def test_laplacian_restatement_matches_reference_fixtures():
         got = OL.local_laplacian(z['frame%d' % n], float(z['alpha']),
                                  float(z['beta']))
         assert np.array_equal(got, z['out%d' % n])
+
+
+# ---------------------------------------------------------------------------
+# Restatements of the pipelines the reference ships no generated code for,
+# pinned to the reference's own DSL specs evaluated point by point
+# (fixtures written by tests/golden/make_spec_golden.py).
+
+def test_campipe_restatement_matches_reference_spec():
+    """oracle/campipe.c equals the reference's camera_pipe spec evaluated
+    with C semantics, byte for byte, at two parameter sets; its const
+    tables equal the spec's matrix and all 65536 curve entries."""
+    import oracle.campipe as OC
+    z = np.load(os.path.join(GOLD, "campipe_spec.npz"))
+    for n in range(2):
+        kelvin, contrast, gamma = (float(v) for v in z['params%d' % n])
+        got = OC.campipe(z['img%d' % n], kelvin, contrast, gamma)
+        assert np.array_equal(got, z['out%d' % n])
+    mat, lut = OC.tables(*(float(v) for v in z['params0']))
+    assert np.array_equal(mat, z['matrix'])
+    assert np.array_equal(lut, z['lut'])
+
+
+def test_bilateral_restatement_matches_reference_spec():
+    """oracle/bilateral.py equals the reference's bilateral_grid spec in
+    FP64 (bins as compiled) to FP64 round-off; the reference's own float
+    arithmetic stays within 1e-5 of it."""
+    import oracle.bilateral as OB
+    z = np.load(os.path.join(GOLD, "bilateral_spec.npz"))
+    for n in range(2):
+        got = OB.bilateral(z['img%d' % n])
+        assert np.abs(got - z['fp64%d' % n]).max() <= 1e-12
+        assert np.abs(got - z['f32%d' % n]).max() <= 1e-5
+
+
+def test_pyramid_restatement_matches_reference_spec():
+    """oracle/pyramid.py (L = 4) equals the reference's pyramid_blending
+    spec in FP64 over the spec's output box; the reference's own float
+    arithmetic stays within 1e-6 of it."""
+    import oracle.pyramid as OP
+    z = np.load(os.path.join(GOLD, "pyramid_spec.npz"))
+    for n in range(2):
+        R, C = (int(v) for v in z['shape%d' % n])
+        i1, i2, m = OP.make_inputs(R, C, seed=R)
+        got = OP.pyramid_blend(i1, i2, m)
+        (x0, x1), (y0, y1) = OP.output_box(R, C)
+        assert tuple(z['lo%d' % n]) == (0, x0, y0)
+        assert got.shape == z['fp64%d' % n].shape
+        assert np.abs(got - z['fp64%d' % n]).max() <= 1e-12
+        assert np.abs(got - z['f32%d' % n]).max() <= 1e-6
