@@ -1,0 +1,31 @@
+/* pipeline_Vcycle3d -- C ABI of the PolyMage pipeline 'Vcycle3d' built for NVIDIA B200 (sm_100a).
+ * Generated by polymage_b200; argument order: parameters, then inputs, then
+ * outputs, each sorted by name.  pipeline_Vcycle3d replaces the function of the same
+ * name the reference generates (signature built at sandbox/codegen.py:957-1007,
+ * sandbox/targetc.py:344-366; called through ctypes as in sandbox/apps/python/
+ * img_proc/harris/exec_pipe.py:13-35); the other entry points are additions. */
+#pragma once
+#ifdef __cplusplus
+extern "C" {
+#endif
+/* host buffers, synchronous (reference ABI) */
+void pipeline_Vcycle3d(int n, void* F_, void* V_, void* Vcycle3d);
+/* device buffers, asynchronous on `stream` (cudaStream_t); returns a PM status */
+int pipeline_Vcycle3d_dev(int n, void* F_, void* V_, void* Vcycle3d, void* stream);
+/* same as _dev through a CUDA graph captured on first use */
+int pipeline_Vcycle3d_graph(int n, void* F_, void* V_, void* Vcycle3d, void* stream);
+/* n images; iparams: n x 1 int params, fparams: n x 0 float params, each row in
+ * name order; inputs: n x 2 device pointers, outputs: n x 1 device pointers */
+int pipeline_Vcycle3d_batch(int n, const int* iparams, const float* fparams, void* const* inputs, void* const* outputs, void* stream);
+/* same as _batch through a CUDA graph captured on first use (re-captured when
+ * the arguments change); a repeated _batch call with unchanged arguments
+ * relaunches kernels only */
+int pipeline_Vcycle3d_batch_graph(int n, const int* iparams, const float* fparams, void* const* inputs, void* const* outputs, void* stream);
+/* status of the last call: 0 ok, 1 bad parameters, 2 CUDA error, 3 kernel error */
+int pipeline_Vcycle3d_status(void);
+/* synchronizes and reports the device error word */
+int pipeline_Vcycle3d_check(void);
+void pipeline_Vcycle3d_clear_error(void);
+#ifdef __cplusplus
+}
+#endif

@@ -1,6 +1,9 @@
 /* pipeline_laplacian -- C ABI of the PolyMage pipeline 'laplacian' built for NVIDIA B200 (sm_100a).
  * Generated by polymage_b200; argument order: parameters, then inputs, then
- * outputs, each sorted by name (the reference's generated pipeline_<name> ABI). */
+ * outputs, each sorted by name.  pipeline_laplacian replaces the function of the same
+ * name the reference generates (signature built at sandbox/codegen.py:957-1007,
+ * sandbox/targetc.py:344-366; called through ctypes as in sandbox/apps/python/
+ * img_proc/harris/exec_pipe.py:13-35); the other entry points are additions. */
 #pragma once
 #ifdef __cplusplus
 extern "C" {

@@ -25,6 +25,10 @@ from .campipe import build_campipe
 from .bilateral_grid import build_bilateral
 from .pyramid_blend import build_pyramid, build_pyramid_clamped
 from .local_laplacian import build_laplacian
+from .interpolate import build_interpolate
+from .jacobi import build_jacobi2d, build_jacobi3d
+from .multigrid import build_v_cycle
+from .nas_mg import build_mg3p
 
 HARRIS = dict(tile_sizes=(16, 128), group_size=11,
               options=('rblock=8', 'min_blocks=4'))
@@ -43,6 +47,23 @@ PYRAMID8 = dict(L=8, tile_sizes=(32, 64), group_size=10,
 # local Laplacian filter (the video demo's pipeline_laplacian), 1080p frames
 LAPLACIAN = dict(tile_sizes=(32, 64), group_size=10, options=('rblock=8',))
 
+# The widening pipelines at the reference Makefiles' settings: Jacobi 2-D
+# N=2048 and 3-D N=128 with 10 steps each (stencil/jacobi{2D,3D}/
+# Makefile:10-11), multigrid cycles with L=3 levels above a 31-point coarse
+# grid, 10 pre-smoothings and none after or on the coarsest level
+# (multigrid/jacobi{2D,3D}/Makefile:10-16), NAS MG class W (NAS-PB-MG-3.2/
+# Makefile:9), interpolation of a 2048x2048 RGBA image.
+INTERPOLATE = dict(rows=2048, cols=2048, tile_sizes=(16, 16), group_size=11)
+JACOBI2D = dict(N=2048, T=10, tile_sizes=(16, 64), group_size=10)
+JACOBI3D = dict(N=128, T=10, tile_sizes=(4, 8, 32), group_size=5)
+VCYCLE = dict(n=31, L=3, nu1=10, nu2=0, nuc=0, tile_sizes=(16, 64),
+              group_size=6)
+WCYCLE = dict(VCYCLE, gamma=2, name="Wcycle")
+VCYCLE3D = dict(n=31, L=3, nu1=10, nu2=0, nuc=0, dims=3,
+                tile_sizes=(4, 8, 32), group_size=4, name="Vcycle3d")
+WCYCLE3D = dict(VCYCLE3D, gamma=2, name="Wcycle3d")
+MG3P = dict(prob_class='W', tile_sizes=(4, 8, 32), group_size=6)
+
 _BUILDERS = {
     "harris": (build_harris, HARRIS),
     "unsharp": (build_unsharp, UNSHARP),
@@ -51,6 +72,14 @@ _BUILDERS = {
     "pyramid": (build_pyramid, PYRAMID),
     "pyramid8": (build_pyramid_clamped, PYRAMID8),
     "laplacian": (build_laplacian, LAPLACIAN),
+    "interpolate": (build_interpolate, INTERPOLATE),
+    "jacobi2d": (build_jacobi2d, JACOBI2D),
+    "jacobi3d": (build_jacobi3d, JACOBI3D),
+    "vcycle": (build_v_cycle, VCYCLE),
+    "wcycle": (build_v_cycle, WCYCLE),
+    "vcycle3d": (build_v_cycle, VCYCLE3D),
+    "wcycle3d": (build_v_cycle, WCYCLE3D),
+    "mg3p": (build_mg3p, MG3P),
 }
 
 _cache = {}

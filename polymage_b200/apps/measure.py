@@ -23,6 +23,11 @@ from . import catalog
 
 APPS = ("harris", "unsharp", "campipe", "bilateral", "pyramid", "pyramid8",
         "laplacian")
+# the pipelines beyond the benchmark configurations, at the reference
+# Makefiles' sizes (catalog); for the grids "pixels" are the interior
+# points a call updates
+WIDENING = ("interpolate", "jacobi2d", "jacobi3d", "vcycle", "wcycle",
+            "vcycle3d", "wcycle3d", "mg3p")
 FLUSH_BYTES = 256 << 20
 
 
@@ -84,6 +89,43 @@ def workload(app, seed=0):
                 {'laplacian': ((H, W, 3), np.uint8)}, H * W,
                 "local_laplacian 1920x1080 uint8 BGR, 4 intensity levels, "
                 "5 pyramid levels")
+    if app == 'interpolate':
+        R = C = 2048
+        img = np.zeros((4, R + 2, C + 2), np.float32)
+        img[0:3, 1:R + 1, 1:C + 1] = rng.random((3, R, C), dtype=np.float32)
+        img[3, 1:R + 1, 1:C + 1] = 0.25 + 0.75 * rng.random(
+            (R, C), dtype=np.float32)
+        return ({'R': R, 'C': C}, {'img': img},
+                {'interpolate': ((3, R, C), np.float32)}, R * C,
+                "interpolate 2048x2048 RGBA float32, 10 levels")
+    if app in ('jacobi2d', 'jacobi3d'):
+        kw = catalog.JACOBI2D if app == 'jacobi2d' else catalog.JACOBI3D
+        N, dims = kw['N'], 2 if app == 'jacobi2d' else 3
+        shape = (N + 2,) * dims
+        return ({'N': N}, {'V_': rng.random(shape), 'F_': rng.random(shape)},
+                {'jacobi': (shape, np.float64)}, N ** dims,
+                "jacobi %dD N=%d float64, %d steps" % (dims, N, kw['T']))
+    if app in ('vcycle', 'wcycle', 'vcycle3d', 'wcycle3d'):
+        kw = catalog._BUILDERS[app][1]
+        n, L, dims = kw['n'], kw['L'], kw.get('dims', 2)
+        N = (n + 1) * (1 << L) - 1
+        shape = (N + 2,) * dims
+        out = {'vcycle': 'Vcycle', 'wcycle': 'Wcycle',
+               'vcycle3d': 'Vcycle3d', 'wcycle3d': 'Wcycle3d'}[app]
+        return ({'n': n}, {'V_': rng.random(shape), 'F_': rng.random(shape)},
+                {out: (shape, np.float64)}, N ** dims,
+                "%s-cycle %dD finest %d^%d float64, L=%d nu1=%d nu2=%d "
+                "nuc=%d" % ('W' if kw.get('gamma', 1) == 2 else 'V', dims, N,
+                            dims, L, kw['nu1'], kw['nu2'], kw['nuc']))
+    if app == 'mg3p':
+        from .nas_mg import SIZES
+        n = SIZES[catalog.MG3P['prob_class']]
+        shape = (n + 2,) * 3
+        return ({'n': n}, {'U': rng.random(shape), 'V': rng.random(shape),
+                           'R': rng.random(shape)},
+                {'MG_U': (shape, np.float64), 'MG_R': (shape, np.float64)},
+                n ** 3, "NAS MG mg3P class %s (%d^3) float64"
+                % (catalog.MG3P['prob_class'], n))
     raise ValueError(app)
 
 
@@ -97,15 +139,17 @@ def hbm_peak():
     return 6650.0, "fallback"
 
 
-def measure(app, steps=50, warmup=5, device=None, graph=True, warm=False):
+def measure(app, steps=50, warmup=5, device=None, graph=True, warm=False,
+            cp=None):
     """Mean device time of ``steps`` runs of one shipped pipeline at its
     benchmark size (CUDA events on the launching stream).  By default 256 MB
     are written before each run so that nothing starts in L2; ``warm``
     leaves the previous run's data in L2 (the sub-L2 workloads' warm
-    numbers)."""
+    numbers).  ``cp``: another build of the same pipeline (a variant of
+    the catalog's) to time instead of the catalog's."""
     import torch
     dev = device or torch.device("cuda", torch.cuda.current_device())
-    cp = catalog.build(app)
+    cp = cp or catalog.build(app)
     prm, host_in, out_spec, pixels, desc = workload(app)
     ins = dict((k, torch.from_numpy(v).to(dev)) for k, v in host_in.items())
     outs = {}
@@ -135,12 +179,15 @@ def measure(app, steps=50, warmup=5, device=None, graph=True, warm=False):
         ev[i][1].record(stream)
     torch.cuda.synchronize(dev)
     cp.check()
-    ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
+    per = sorted(a.elapsed_time(b) for a, b in ev)
+    ms = float(np.mean(per))
     nbytes = sum(v.nbytes for v in host_in.values()) + sum(
         int(np.prod(s)) * np.dtype(d).itemsize for s, d in out_spec.values())
     peak, kind = hbm_peak()
     gbs = nbytes / (ms / 1e3) / 1e9
     return {"app": app, "workload": desc, "ms": ms,
+            "ms_min": per[0], "ms_median": float(np.median(per)),
+            "ms_max": per[-1],
             "mpix_s": pixels / (ms / 1e3) / 1e6,
             "launches": sum({'stencil': 1, 'reduction': 2}.get(g['kind'], 0)
                             for g in cp.module.meta.get('groups', [])),
@@ -261,7 +308,8 @@ def measure_stream(n=1024, seed=1, device=None):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--app", action="append",
-                    choices=APPS + ("bilateral_batch64", "stream1024"))
+                    choices=APPS + WIDENING + ("bilateral_batch64",
+                                               "stream1024"))
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--warm", action="store_true",

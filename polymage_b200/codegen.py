@@ -1492,8 +1492,14 @@ class PipelineGen(object):
             "NVIDIA B200 (sm_100a)." % (name, self.p.name),
             " * Generated by polymage_b200; argument order: parameters, then "
             "inputs, then",
-            " * outputs, each sorted by name (the reference's generated "
-            "pipeline_<name> ABI). */",
+            " * outputs, each sorted by name.  pipeline_%s replaces the "
+            "function of the same" % name,
+            " * name the reference generates (signature built at "
+            "sandbox/codegen.py:957-1007,",
+            " * sandbox/targetc.py:344-366; called through ctypes as in "
+            "sandbox/apps/python/",
+            " * img_proc/harris/exec_pipe.py:13-35); the other entry points "
+            "are additions. */",
             "#pragma once",
             "#ifdef __cplusplus",
             'extern "C" {',
@@ -1696,30 +1702,116 @@ class StencilGen(object):
           '__grid_constant__ %s_launch L)' % (lb, k, k))
         w.open("")
         w("extern __shared__ __align__(128) unsigned char pm_smem[];")
+        # option 'prefetch': the next tile's staged inputs are loaded into
+        # a second copy of their buffers while this tile computes
+        pre = bool(self.stage_nodes) and 'prefetch' in pg.p.options and \
+            getattr(plan, 'stage_delta', 0) > 0
+        self.prefetch = pre
         if self.stage_nodes:
-            # one mbarrier per CTA for the staged inputs, initialized once;
-            # each tile that issues TMA loads completes one phase of it
+            # one mbarrier per copy of the staged inputs, initialized once;
+            # each tile that issues TMA loads completes one phase of the
+            # barrier of its copy (bit k of pm_phase: parity of barrier k)
             w("uint64_t* pm_bar = reinterpret_cast<uint64_t*>(pm_smem + %d);"
               % (plan.smem_bytes - 128))
             w.open("if (threadIdx.x == 0)")
             w("pm_mbar_init(pm_bar, 1);")
+            if pre:
+                w("pm_mbar_init(pm_bar + 1, 1);")
             w("pm_fence_barrier_init();")
             w.close()
             w("__syncthreads();")
             w("uint32_t pm_phase = 0;")
         w("__shared__ int pm_next_tile;")
-        w("// Tiles: blockIdx.x first; with a tile queue (persistent launch)")
-        w("// each CTA then takes the next index from the device counter.")
-        w.open("for (int tile = L.first + (int)blockIdx.x; tile < L.total; )")
+        if not pre:
+            w("// Tiles: blockIdx.x first; with a tile queue (persistent "
+              "launch)")
+            w("// each CTA then takes the next index from the device "
+              "counter.")
+            w.open("for (int tile = L.first + (int)blockIdx.x; tile < "
+                   "L.total; )")
+            self.gen_tile_setup("tile")
+            self.gen_buffers(None)
+            if self.stage_nodes:
+                self.gen_issue("pm_bar")
+                self.gen_coop_loads()
+                self.gen_wait("pm_bar", "0", None)
+            for f in plan.steps:
+                self.gen_step(f)
+            w("if (!L.queue) break;")
+            if self.stage_nodes:
+                w("pm_fence_proxy_async();   // the next tile's TMA rewrites "
+                  "smem")
+            w("__syncthreads();      // shared memory is reused by the next "
+              "tile")
+            w("if (threadIdx.x == 0) pm_next_tile = L.first + (int)gridDim.x"
+              " + atomicAdd(L.queue, 1);")
+            w("__syncthreads();")
+            w("tile = pm_next_tile;")
+            w.close()
+            w.close()
+            w("")
+            return
+        # Prefetching tile loop: the staged inputs of a CTA's tiles
+        # alternate between two copies; the loads of tile n+1 are issued
+        # (thread 0) before tile n is computed.  The next index is drawn
+        # from the queue one tile ahead.
+        w("int pm_buf = 0;          // copy of the staged inputs this tile "
+          "reads")
+        w("int tile = L.first + (int)blockIdx.x;")
+        w("bool pm_pend = false;    // loads in flight into the other copy")
+        w.open("if (tile < L.total)")
+        self.gen_tile_setup("tile")
+        self.gen_stage_ptrs("0")
+        self.gen_issue("pm_bar")
+        w.close()
+        w.open("while (tile < L.total)")
+        w("int pm_nt = L.total;")
+        w.open("if (L.queue)")
+        w("if (threadIdx.x == 0) pm_next_tile = L.first + (int)gridDim.x + "
+          "atomicAdd(L.queue, 1);")
+        w("__syncthreads();")
+        w("pm_nt = pm_next_tile;")
+        w.close()
+        w("pm_pend = false;")
+        w.open("if (pm_nt < L.total)")
+        self.gen_tile_setup("pm_nt")
+        self.gen_stage_ptrs("pm_buf ^ 1")
+        self.gen_issue("pm_bar + (pm_buf ^ 1)")
+        w("pm_pend = any_tma;")
+        w.close()
+        w.open("")
+        self.gen_tile_setup("tile")
+        self.gen_buffers("pm_buf")
+        self.gen_coop_loads()
+        self.gen_wait("pm_bar + pm_buf", "pm_buf", "pm_bar + (pm_buf ^ 1)")
+        for f in plan.steps:
+            self.gen_step(f)
+        w.close()
+        w("pm_fence_proxy_async();   // a later tile's TMA rewrites this copy")
+        w("__syncthreads();")
+        w("pm_buf ^= 1;")
+        w("tile = pm_nt;")
+        w.close()
+        w.close()
+        w("")
+
+    def gen_tile_setup(self, tile):
+        """Descriptor, parameters, tile box, domains and region inference of
+        tile index ``tile`` (emitted into the current scope)."""
+        pg = self.pg
+        plan = self.plan
+        w = pg.w
+        k = self.k
+        na = plan.anchor.ndims
         w("const %s_desc* Dp = &L.d0;" % k)
         w("if (L.nimg > 1) Dp = L.descs + pm_find_image(L.descs, L.nimg, "
-          "tile);")
+          "%s);" % tile)
         w("const %s_desc& D = *Dp;" % k)
         pg.declare_params(w, "D")
         ctx = ExprCtx(w, 'device', pg.pmap, self.reader)
         self.ctx = ctx
         # tile coordinates
-        w("int rem = tile - D.tile_base;")
+        w("int rem = %s - D.tile_base;" % tile)
         for d in range(na - 1, 0, -1):
             w("const int t%d = rem %% D.gn[%d]; rem /= D.gn[%d];" % (d, d, d))
         w("const int t0 = rem;")
@@ -1737,31 +1829,36 @@ class StencilGen(object):
                 pg.declare_domain(w, f, ctx, True)
         # region inference
         self.gen_regions()
-        # buffers
+
+    def gen_buffers(self, buf):
+        """HBM buffer pointers and shared-memory buffers of the current
+        tile; ``buf``: the copy of the staged inputs (prefetch) or None."""
+        pg = self.pg
+        w = pg.w
         for f in self.bufs:
             w("%s%s* __restrict__ b_%s = D.b_%s;" % (
                 "" if any(f is n.func for n in self.outs) else "const ",
                 ctype(f.typ), pg.fn(f), pg.fn(f)))
-        for n in plan.nodes:
+        for n in self.plan.nodes:
             if n.in_smem:
+                if n.role == 'stage' and buf is not None:
+                    self.gen_stage_ptrs(buf, [n])
+                    continue
                 nm = self.node_name(n)
                 w("%s* sm_%s = reinterpret_cast<%s*>(pm_smem + %d);" % (
                     ctype(n.func.typ), nm, ctype(n.func.typ), n.smem_off))
                 self.decl_smem_origin(n)
-        self.gen_staging()
-        for f in plan.steps:
-            self.gen_step(f)
-        w("if (!L.queue) break;")
-        if self.stage_nodes:
-            w("pm_fence_proxy_async();   // the next tile's TMA rewrites smem")
-        w("__syncthreads();      // shared memory is reused by the next tile")
-        w("if (threadIdx.x == 0) pm_next_tile = L.first + (int)gridDim.x + "
-          "atomicAdd(L.queue, 1);")
-        w("__syncthreads();")
-        w("tile = pm_next_tile;")
-        w.close()
-        w.close()
-        w("")
+
+    def gen_stage_ptrs(self, buf, nodes=None):
+        """Shared-memory pointers and origins of the staged inputs in copy
+        ``buf`` (0 or 1) of their buffers."""
+        w = self.pg.w
+        for n in (self.stage_nodes if nodes is None else nodes):
+            nm = self.node_name(n)
+            t = ctype(n.func.typ)
+            w("%s* sm_%s = reinterpret_cast<%s*>(pm_smem + %d + (%s) * %d);"
+              % (t, nm, t, n.smem_off, buf, self.plan.stage_delta))
+            self.decl_smem_origin(n)
 
     def empty_expr(self, n, kind="r"):
         nm = self.node_name(n)
@@ -2139,15 +2236,14 @@ class StencilGen(object):
             first = False
 
     # ---- staging of external producers ------------------------------------------
-    def gen_staging(self):
+    def gen_issue(self, bar):
+        """TMA loads of the staged inputs of the tile set up in this scope,
+        completing on mbarrier ``bar`` (thread 0 issues them); declares
+        ``any_tma``."""
         pg = self.pg
-        plan = self.plan
         w = pg.w
-        stage_nodes = self.stage_nodes
-        if not stage_nodes:
-            return
         conds = []
-        for n in stage_nodes:
+        for n in self.stage_nodes:
             nm = self.node_name(n)
             w("const bool use_tma_%s = D.tma_%s && !(%s);" % (
                 nm, nm, self.empty_expr(n)))
@@ -2155,25 +2251,31 @@ class StencilGen(object):
         w("const bool any_tma = %s;" % " || ".join(conds))
         w.open("if (any_tma && threadIdx.x == 0)")
         w("uint32_t bytes = 0;")
-        for n in stage_nodes:
+        for n in self.stage_nodes:
             nm = self.node_name(n)
             box = 1
             for e in n._sm_ext:
                 box *= e
             w("if (use_tma_%s) bytes += %du;" % (nm, box * n.func.typ.size()))
-        w("pm_mbar_arrive_expect_tx(pm_bar, bytes);")
-        for n in stage_nodes:
+        w("pm_mbar_arrive_expect_tx(%s, bytes);" % bar)
+        for n in self.stage_nodes:
             nm = self.node_name(n)
             fnm = pg.fn(n.func)
             nd = n.ndims
             coords = ["so_%s_%d" % (nm, nd - 1)]
             for d in range(nd - 2, -1, -1):
                 coords.append("r_%s_lo%d - d_%s_lo%d" % (nm, d, fnm, d))
-            w("if (use_tma_%s) pm_tma_load_%dd(sm_%s, &D.tm_%s, pm_bar, %s);"
-              % (nm, nd, nm, nm, ", ".join(coords)))
+            w("if (use_tma_%s) pm_tma_load_%dd(sm_%s, &D.tm_%s, %s, %s);"
+              % (nm, nd, nm, nm, bar, ", ".join(coords)))
         w.close()
-        # cooperative fallback
-        for n in stage_nodes:
+
+    def gen_coop_loads(self):
+        """Cooperative loads of the staged inputs that have no tensor map
+        (unaligned buffers), into the current tile's copy."""
+        pg = self.pg
+        plan = self.plan
+        w = pg.w
+        for n in self.stage_nodes:
             nm = self.node_name(n)
             fnm = pg.fn(n.func)
             nd = n.ndims
@@ -2201,11 +2303,30 @@ class StencilGen(object):
                 ctype(n.func.typ)))
             w.close()
             w.close()
-        w.open("if (any_tma)")
-        w("pm_mbar_wait(pm_bar, pm_phase, &pm_err_word);")
-        w("pm_phase ^= 1u;")
+
+    def gen_wait(self, bar, bit, other):
+        """Wait for the current tile's TMA loads on ``bar`` (phase bit
+        ``bit`` of pm_phase), then a CTA barrier.  If any thread's bounded
+        wait ran out (the error word records it), the CTA computes nothing
+        more: it waits, again bounded, for loads in flight into the other
+        copy (``other``, prefetch), and returns."""
+        pg = self.pg
+        w = pg.w
+        w("const bool any_tma_cur = %s;" % " || ".join(
+            "(D.tma_%s && !(%s))" % (self.node_name(n), self.empty_expr(n))
+            for n in self.stage_nodes))
+        w("bool pm_fail = false;")
+        w.open("if (any_tma_cur)")
+        w("pm_fail = !pm_mbar_wait(%s, (pm_phase >> (%s)) & 1u, "
+          "&pm_err_word);" % (bar, bit))
+        w("pm_phase ^= 1u << (%s);" % bit)
         w.close()
-        w("__syncthreads();")
+        w.open("if (__syncthreads_or(pm_fail))")
+        if other is not None:
+            w("if (pm_pend) pm_mbar_wait(%s, (pm_phase >> (%s ^ 1)) & 1u, "
+              "nullptr);" % (other, bit))
+        w("return;")
+        w.close()
 
     def decompose(self, iv, ext, prefix):
         w = self.pg.w

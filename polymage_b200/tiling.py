@@ -537,7 +537,8 @@ def plan_stencil(pipeline, comps):
 
     _static_extents(plan, env)
     _alignment(plan, env)
-    _layout_smem(plan, tight=('tight_stage' in pipeline.options), env=env)
+    _layout_smem(plan, tight=('tight_stage' in pipeline.options), env=env,
+                 prefetch=('prefetch' in pipeline.options))
     if plan.smem_bytes > int(_option(pipeline, 'smem_budget', SMEM_BUDGET)):
         raise PlanError("shared memory %d B exceeds budget" %
                         plan.smem_bytes)
@@ -847,14 +848,20 @@ def _alignment(plan, env):
                     raise PlanError("inconsistent scaling of %s" % n.name)
 
 
-def _layout_smem(plan, tight=False, env=None):
+def _layout_smem(plan, tight=False, env=None, prefetch=False):
     """Shared-memory buffers, placed first-fit by lifetime.  A staged
     input's rows carry the slack a TMA box needs when its origin is
     rounded down to 16 bytes; with ``tight`` (option 'tight_stage') an
     input whose innermost dimension is staged whole and is narrower than
     16 bytes (the channels of an interleaved uint8 image), which no tensor
     map can describe, gets rows of exactly that width: its origin offset
-    is then always 0 and the cooperative loads cover only used bytes."""
+    is then always 0 and the cooperative loads cover only used bytes.
+
+    With ``prefetch`` (option 'prefetch': a CTA loads its next tile's
+    staged inputs while it computes the current tile) staged inputs live
+    for the whole tile, so that no stage buffer shares their bytes, and
+    get a second copy ``plan.stage_delta`` bytes above the first; the
+    tiles of a CTA alternate between the two copies."""
     bufs = []
     for n in plan.nodes:
         if not n.in_smem:
@@ -884,6 +891,13 @@ def _layout_smem(plan, tight=False, env=None):
             nbytes *= e
         n.smem_bytes = ((nbytes + 127) // 128) * 128
         bufs.append(n)
+    plan.stage_delta = 0
+    staged = [n for n in bufs if n.role == 'stage'] if prefetch else []
+    end = max([n.last_step for n in bufs] or [0])
+
+    def life(q):
+        return (q.step, end if q in staged else q.last_step)
+
     placed = []
     total = 0
     for n in sorted(bufs, key=lambda q: (q.step, -q.smem_bytes)):
@@ -891,8 +905,8 @@ def _layout_smem(plan, tight=False, env=None):
         while True:
             clash = None
             for p in placed:
-                overlap_t = not (p.last_step < n.step or
-                                 n.last_step < p.step)
+                overlap_t = not (life(p)[1] < life(n)[0] or
+                                 life(n)[1] < life(p)[0])
                 overlap_m = off < p.smem_off + p.smem_bytes and \
                     p.smem_off < off + n.smem_bytes
                 if overlap_t and overlap_m:
@@ -904,6 +918,10 @@ def _layout_smem(plan, tight=False, env=None):
         n.smem_off = off
         placed.append(n)
         total = max(total, off + n.smem_bytes)
+    if staged:
+        plan.stage_delta = ((total + 127) // 128) * 128
+        total = plan.stage_delta + max(n.smem_off + n.smem_bytes
+                                       for n in staged)
     plan.smem_bytes = total + 128       # + mbarrier / flags area
 
 

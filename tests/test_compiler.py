@@ -330,14 +330,30 @@ def _next_app(name):
         from polymage_b200.apps.multigrid import build_v_cycle
         return (build_v_cycle(n=7, L=2, dims=3, gamma=2, name="Wcycle3d",
                               tile_sizes=(4, 8, 32)), {'n': 7})
+    if name.startswith("catalog:"):
+        # the catalog's builds at sizes the GPU tests run them at
+        from polymage_b200.apps import catalog
+        app, size = name[len("catalog:"):].split("@")
+        b, kw = catalog._BUILDERS[app]
+        key = {"interpolate": "R", "mg3p": "n"}.get(app, "N")
+        if app.endswith("cycle") or app.endswith("cycle3d"):
+            key = "n"
+        sizes = {key: int(size)}
+        if app == "interpolate":
+            sizes = {'R': int(size), 'C': int(size) * 3 // 4 + 1}
+        return b(**kw), sizes
     from polymage_b200.apps.nas_mg import build_mg3p
     return build_mg3p('S'), {'n': 32}
 
 
-@pytest.mark.parametrize("name", ["interpolate", "jacobi2d", "vcycle",
-                                  "wcycle3d", "nas_mg"])
+@pytest.mark.parametrize("name", [
+    "interpolate", "jacobi2d", "vcycle", "wcycle3d", "nas_mg",
+    "catalog:interpolate@211", "catalog:jacobi2d@333",
+    "catalog:jacobi3d@47", "catalog:vcycle@20", "catalog:wcycle@13",
+    "catalog:vcycle3d@8", "catalog:wcycle3d@6", "catalog:mg3p@128"])
 def test_static_extents_cover_every_tile_next_apps(name):
-    """The same tile-by-tile check for the apps not yet run on a GPU."""
+    """The same tile-by-tile check for the widening apps, at sizes their
+    GPU tests run."""
     p, sizes = _next_app(name)
     env = p.int_env()
     for k in list(env):
