@@ -16,9 +16,13 @@ Reported (one JSON line, rank 0):
   cpu_baseline  the reference's own generated C++ (pipeline_mask, OpenMP on
             all host cores) on a bounded sample of the same workload
   clocks    SM clocks and throttle reasons sampled during the timed region
-  pipelines every shipped pipeline (Harris, unsharp, camera pipe, bilateral
-            grid, pyramid blending) at its benchmark size: MPix/s and the
-            compulsory-bytes HBM roofline fraction (polymage_b200.apps.measure)
+  pipelines every shipped pipeline (the five benchmark configurations, the
+            local Laplacian and the widening pipelines) at its benchmark
+            size: MPix/s, the compulsory-bytes HBM roofline fraction and the
+            spread of its run times (polymage_b200.apps.measure); with the
+            cpu_baseline leg also its error against the oracle on the same
+            inputs and its CPU baseline on all host cores and on one
+            (oracle/baselines.py)
 
 ``--impl reference`` times the reference's CPU implementation alone.
 Multi-GPU (torchrun): every rank runs its own image (replicas, weak
@@ -159,6 +163,46 @@ def cpu_baseline(budget_s=3.0):
                       "best of %d" % (len(ts), R, C, len(ts))}
 
 
+def pipeline_check(app, dev):
+    """The cpu_baseline leg for one shipped pipeline at its benchmark size:
+    its output on the GPU (host-buffer entry) against the oracle on the
+    same inputs (``error``), and the CPU baseline timed on all host cores
+    and on one (``cpu_baseline``; oracle/baselines.py says which
+    implementation each pipeline has)."""
+    from polymage_b200.apps import catalog, measure
+    import oracle.baselines as OBL
+    cp = catalog.build(app)
+    prm, host_in, out_spec, pixels, desc = measure.workload(app)
+    outs = dict((k, np.zeros(sh, dt)) for k, (sh, dt) in out_spec.items())
+    cp.run_host(prm, host_in, outs)
+    exp, masks, base = OBL.check_and_time(app, prm, host_in, os.cpu_count())
+    err = {}
+    for k, ref in exp.items():
+        got = outs[k]
+        m = masks.get(k)
+        integer = np.issubdtype(got.dtype, np.integer)
+        d = np.abs(got.astype(np.float64) - np.asarray(ref, np.float64))
+        scale = float(np.abs(ref).max()) or 1.0
+        sel = d if m is None else d[m]
+        e = {"max_abs": float(sel.max()),
+             "max_abs_over_max_ref": float(sel.max()) / scale}
+        if integer:
+            e["mismatched"] = int(np.count_nonzero(sel))
+            e["of"] = int(sel.size)
+        else:
+            r = np.abs(np.asarray(ref, np.float64))
+            rel = d / np.maximum(r, 1e-6 * scale)
+            e["max_rel_floor_1e-6"] = float((rel if m is None else
+                                             rel[m]).max())
+        if m is not None:
+            e["tie_band_excluded"] = int(m.size - np.count_nonzero(m))
+        err[k] = e
+    for b in base.values():
+        b["value"] = pixels / b["seconds"] / 1e6
+        b["unit"] = "MPix/s"
+    return {"error": err, "cpu_baseline": base}
+
+
 def run_reference_arm(args):
     ws, rank = _dist()
     if rank != 0:
@@ -270,7 +314,8 @@ def run(args):
     clk = clocks.stop() if clocks else None
     cp.check()
     elapsed_ms = t0.elapsed_time(t1)
-    kern_ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
+    per_step = sorted(a.elapsed_time(b) for a, b in ev)
+    kern_ms = float(np.mean(per_step))
     elapsed_ms = max_over_ranks(elapsed_ms, dev, ws)
     value = job_rate(args.steps * R * C, ws, elapsed_ms / 1e3) / 1e6
 
@@ -319,7 +364,10 @@ def run(args):
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_kind,
                          "alg_bytes_per_launch": ALG_BYTES,
-                         "kernel_ms": kern_ms},
+                         "kernel_ms": kern_ms,
+                         "kernel_ms_min": per_step[0],
+                         "kernel_ms_median": float(np.median(per_step)),
+                         "kernel_ms_max": per_step[-1]},
             "gpu_launches": args.steps,
             "clocks": clk,
         }
@@ -330,13 +378,17 @@ def run(args):
             from polymage_b200.apps import measure
             line["pipelines"] = dict(
                 (a, measure.measure(a, steps=50, warmup=5, device=dev))
-                for a in measure.APPS)
+                for a in measure.APPS + measure.WIDENING)
             line["pipelines"]["bilateral_batch64"] = \
                 measure.measure_bilateral_batch(64, device=dev)
             line["pipelines"]["stream1024"] = measure.measure_stream(
                 1024, device=dev)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline()
+            if "pipelines" in line:
+                for app, entry in line["pipelines"].items():
+                    if app in measure.APPS + measure.WIDENING:
+                        entry.update(pipeline_check(app, dev))
         print(json.dumps(line))
     if ws > 1:
         dist.barrier()

@@ -42,7 +42,9 @@ int pm_mlp_backward(const float* params, int D, int H, const float* X,
  * H = 128); larger requests return 1 and launch nothing.  The first call on
  * each device looks up the array's address (make it before any stream
  * capture).  Nothing needs to start at zero.  Calls on one device share the
- * array: two in flight at once race, so issue them on one stream. */
+ * array: two in flight at once race, so issue them on one stream.  The
+ * address looked up on a device does not survive a cudaDeviceReset of that
+ * device: do not call this entry on a device after resetting it. */
 int pm_mlp_forward_static(const float* params, int D, int H, const float* X,
                           int B, float* out, void* stream);
 

@@ -246,6 +246,10 @@ class ExprCtx(object):
                 sm = self._static_mod(e, bind)
                 if sm is not None:
                     return str(sm)
+            if e.op == '/':
+                sd = self._static_div(e, bind)
+                if sd is not None:
+                    return sd
             if e.op in ('/', '%') and self._unsigned_ok(e, bind):
                 # truncating division of a non-negative int by a positive
                 # constant equals unsigned division (a shift or mask for
@@ -350,6 +354,33 @@ class ExprCtx(object):
             total += c * rm[0]
         return total % m
 
+    def _static_div(self, e, bind):
+        """``(q + c) / k`` as ``q / k + d`` when the residue of loop variable
+        ``q`` modulo ``k`` is known and the numerator cannot be negative
+        (then q / k + (q % k + c) / k with the second term a constant), so
+        that the consecutive points of a thread that fall into the same
+        cell of a decimated producer index it by the same text; else
+        None."""
+        if not self.var_res:
+            return None
+        r = e.right
+        if not (isinstance(r, Value) and r.typ in _INT_T and
+                int(r.value) > 0) or not self._unsigned_ok(e, bind):
+            return None
+        k = int(r.value)
+        f = affine_form(_subst(e.left, bind))
+        if f is None or len(f[0]) != 1:
+            return None
+        (v, c), = f[0].items()
+        name = getattr(v, '_cname', None)
+        rm = self.var_res.get(name)
+        lo = self.var_lo.get(name)
+        if c != 1 or rm is None or rm[1] % k or lo is None or lo < 0:
+            return None
+        d = (rm[0] % k + f[1]) // k
+        base = "((int)((unsigned)(%s) / %du))" % (name, k)
+        return base if d == 0 else "(%s + %d)" % (base, d)
+
     def _static_int(self, e, bind):
         e = Value.numericToValue(e)
         if isinstance(e, Value):
@@ -433,6 +464,32 @@ class ExprCtx(object):
             s = " + ".join(parts).replace("+ -", "- ")
             return "(%s)" % s
         return self.expr(e, {})
+
+
+def _inner_parity(f, var):
+    """Whether a stage's definition divides or takes the remainder of an
+    expression of ``var`` by 2 (an upsampling by 2 along that dimension)."""
+    from .pipe import body_parts
+    stack = []
+    for cond, expr, red in body_parts(f):
+        stack.append(expr)
+        if cond is not None:
+            stack.append(cond)
+    while stack:
+        x = stack.pop()
+        x = Value.numericToValue(x)
+        if isinstance(x, AbstractBinaryOpNode) and x.op in ('/', '%') and \
+                isinstance(x.right, Value) and x.right.typ in _INT_T and \
+                int(x.right.value) == 2 and \
+                any(v is var for v in x.left.collect(C.Variable)):
+            return True
+        if isinstance(x, C.Condition):
+            stack += [x.lhs, x.rhs]
+        elif hasattr(x, 'children'):
+            stack.extend(x.children())
+        elif isinstance(x, C.Select):
+            stack += [x.condition, x.true_expression, x.false_expression]
+    return False
 
 
 def _opt(pipeline, name, default=None):
@@ -910,10 +967,11 @@ class PipelineGen(object):
         w.close()
         w("")
         # ---- graph replay ----
-        w("static cudaGraphExec_t pm_graph_exec = nullptr;")
-        w("static pm_args pm_graph_key;")
-        w("static void* pm_graph_ws = nullptr;")
-        w("static cudaStream_t pm_graph_stream = nullptr;")
+        w("// per device: the graph, its arguments, workspace and stream")
+        w("static cudaGraphExec_t pm_graph_exec[64];")
+        w("static pm_args pm_graph_key[64];")
+        w("static void* pm_graph_ws[64];")
+        w("static cudaStream_t pm_graph_stream[64];")
         w("// Replays a CUDA graph of the whole pipeline; the graph is")
         w("// (re)captured when the arguments or the workspace change.")
         w.open('extern "C" int pipeline_%s_graph(%s, void* stream)' % (name,
@@ -933,39 +991,38 @@ class PipelineGen(object):
         w("pm_args A; memset(&A, 0, sizeof(A));")
         for line in call_fill:
             w(line)
-        w("int dev = 0; cudaGetDevice(&dev);")
-        w("void* wsnow = (dev >= 0 && dev < 64) ? pm_ws_arena.ptr[dev] : "
-          "nullptr;")
-        w.open("if (!pm_graph_exec || wsnow != pm_graph_ws || memcmp(&A, "
-               "&pm_graph_key, sizeof(A)) != 0)")
+        w("const int dev = pm_cur_dev();")
+        w("void* wsnow = pm_ws_arena.ptr[dev];")
+        w.open("if (!pm_graph_exec[dev] || wsnow != pm_graph_ws[dev] || "
+               "memcmp(&A, &pm_graph_key[dev], sizeof(A)) != 0)")
         w("pm_args B = A;")
         w("int st = pm_run(B, (cudaStream_t)stream);  // sizes workspace, "
           "uploads tables")
         w("if (st) return pm_status = st;")
         w("if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) "
           "return pm_status = PM_ERR_CUDA;")
-        w("if (!pm_graph_stream && cudaStreamCreateWithFlags(&pm_graph_stream,"
-          " cudaStreamNonBlocking) != cudaSuccess) return pm_status = "
-          "PM_ERR_CUDA;")
-        w("if (pm_graph_exec) { cudaGraphExecDestroy(pm_graph_exec); "
-          "pm_graph_exec = nullptr; }")
+        w("if (!pm_graph_stream[dev] && cudaStreamCreateWithFlags("
+          "&pm_graph_stream[dev], cudaStreamNonBlocking) != cudaSuccess) "
+          "return pm_status = PM_ERR_CUDA;")
+        w("if (pm_graph_exec[dev]) { cudaGraphExecDestroy("
+          "pm_graph_exec[dev]); pm_graph_exec[dev] = nullptr; }")
         w("cudaGraph_t g = nullptr;")
-        w("if (cudaStreamBeginCapture(pm_graph_stream, "
+        w("if (cudaStreamBeginCapture(pm_graph_stream[dev], "
           "cudaStreamCaptureModeThreadLocal) != cudaSuccess) return "
           "pm_status = PM_ERR_CUDA;")
         w("pm_args Cc = A;")
-        w("st = pm_run(Cc, pm_graph_stream);")
-        w("cudaError_t e = cudaStreamEndCapture(pm_graph_stream, &g);")
+        w("st = pm_run(Cc, pm_graph_stream[dev]);")
+        w("cudaError_t e = cudaStreamEndCapture(pm_graph_stream[dev], &g);")
         w("if (st || e != cudaSuccess) { if (g) cudaGraphDestroy(g); "
           "cudaGetLastError(); return pm_status = st ? st : PM_ERR_CUDA; }")
-        w("e = cudaGraphInstantiate(&pm_graph_exec, g, 0);")
+        w("e = cudaGraphInstantiate(&pm_graph_exec[dev], g, 0);")
         w("cudaGraphDestroy(g);")
-        w("if (e != cudaSuccess) { pm_graph_exec = nullptr; return "
+        w("if (e != cudaSuccess) { pm_graph_exec[dev] = nullptr; return "
           "pm_status = PM_ERR_CUDA; }")
-        w("pm_graph_key = A;")
-        w("pm_graph_ws = pm_ws_arena.ptr[dev];")
+        w("pm_graph_key[dev] = A;")
+        w("pm_graph_ws[dev] = pm_ws_arena.ptr[dev];")
         w.close()
-        w("if (cudaGraphLaunch(pm_graph_exec, (cudaStream_t)stream) != "
+        w("if (cudaGraphLaunch(pm_graph_exec[dev], (cudaStream_t)stream) != "
           "cudaSuccess) return pm_status = PM_ERR_CUDA;")
         w("return pm_status = PM_OK;")
         w.close()
@@ -1139,11 +1196,11 @@ class PipelineGen(object):
         w("pm_band_ready[dev] = true;")
         w.close()
         w("cudaStream_t sin = pm_band_in[dev], sout = pm_band_out[dev];")
-        w.open("if (!%s_attr)" % k)
+        w.open("if (!%s_attr[pm_cur_dev()])" % k)
         w("if (cudaFuncSetAttribute(%s, cudaFuncAttributeMaxDynamicShared"
           "MemorySize, %d) != cudaSuccess) { pm_status = PM_ERR_CUDA; "
           "return; }" % (k, plan.smem_bytes))
-        w("%s_attr = true;" % k)
+        w("%s_attr[pm_cur_dev()] = true;" % k)
         w.close()
         w("// the kernel's first band must not start before earlier work on s")
         w("cudaEventRecord(pm_band_ev[dev][PM_MAX_BANDS * 2], s);")
@@ -1359,9 +1416,9 @@ class PipelineGen(object):
           len(self.fparams))
         w("pm_key_add(key, inputs, sizeof(void*) * (size_t)n * %d);" % nin)
         w("pm_key_add(key, outputs, sizeof(void*) * (size_t)n * %d);" % nout)
-        w("int dev = 0; cudaGetDevice(&dev);")
-        w.open("if (key == pm_batch_key && pm_batch_ws && dev >= 0 && dev < 64"
-               " && pm_batch_arena.ptr[dev] == pm_batch_ws && "
+        w("const int dev = pm_cur_dev();")
+        w.open("if (key == pm_batch_key && pm_batch_ws && "
+               "pm_batch_arena.ptr[dev] == pm_batch_ws && "
                "pm_batch_tables_current())")
         w("int st = 0;")
         self.emit_calls(w, ["%s(nullptr, nullptr, 0, n, nullptr, nullptr, "
@@ -1399,10 +1456,11 @@ class PipelineGen(object):
           "return pm_status = PM_ERR_CUDA;")
         w("for (int i = 0; i < n; ++i) As[i].ws = (char*)ws;")
         w("char* ddesc = (char*)ws + total;")
-        w("if (!pm_batch_event && cudaEventCreateWithFlags(&pm_batch_event, "
-          "cudaEventDisableTiming) != cudaSuccess) return pm_status = "
-          "PM_ERR_CUDA;")
-        w("cudaEventSynchronize(pm_batch_event);  // previous upload done")
+        w("if (!pm_batch_event[dev] && cudaEventCreateWithFlags("
+          "&pm_batch_event[dev], cudaEventDisableTiming) != cudaSuccess) "
+          "return pm_status = PM_ERR_CUDA;")
+        w("cudaEventSynchronize(pm_batch_event[dev]);  // previous upload "
+          "done")
         w.open("if (pm_batch_pinned_cap < descs_bytes)")
         w("if (pm_batch_pinned) cudaFreeHost(pm_batch_pinned);")
         w("pm_batch_pinned = nullptr; pm_batch_pinned_cap = 0;")
@@ -1417,15 +1475,16 @@ class PipelineGen(object):
                             for f in self.batch_fns],
                         "return pm_status = st;")
         w("// the pinned descriptors are free once every stream's upload is")
-        w("cudaEventRecord(pm_batch_event, s);")
+        w("cudaEventRecord(pm_batch_event[dev], s);")
         w("pm_batch_key = key; pm_batch_ws = ws;")
         w("return pm_status = PM_OK;")
         w.close()
         w("")
-        w("static cudaGraphExec_t pm_bgraph_exec = nullptr;")
-        w("static std::vector<char> pm_bgraph_key;")
-        w("static void* pm_bgraph_ws = nullptr;")
-        w("static cudaStream_t pm_bgraph_stream = nullptr;")
+        w("// per device: the batch graph, its arguments, workspace, stream")
+        w("static cudaGraphExec_t pm_bgraph_exec[64];")
+        w("static std::vector<char> pm_bgraph_key[64];")
+        w("static void* pm_bgraph_ws[64];")
+        w("static cudaStream_t pm_bgraph_stream[64];")
         w("// The batch as one CUDA graph: captured on first use (after one")
         w("// ordinary call has sized the workspace and uploaded descriptors),")
         w("// re-captured when the arguments change.")
@@ -1448,37 +1507,37 @@ class PipelineGen(object):
           len(self.fparams))
         w("pm_key_add(key, inputs, sizeof(void*) * (size_t)n * %d);" % nin)
         w("pm_key_add(key, outputs, sizeof(void*) * (size_t)n * %d);" % nout)
-        w("int dev = 0; cudaGetDevice(&dev);")
-        w("void* wsnow = (dev >= 0 && dev < 64) ? pm_batch_arena.ptr[dev] : "
-          "nullptr;")
-        w.open("if (!pm_bgraph_exec || key != pm_bgraph_key || wsnow != "
-               "pm_bgraph_ws || !pm_batch_tables_current())")
+        w("const int dev = pm_cur_dev();")
+        w("void* wsnow = pm_batch_arena.ptr[dev];")
+        w.open("if (!pm_bgraph_exec[dev] || key != pm_bgraph_key[dev] || "
+               "wsnow != pm_bgraph_ws[dev] || !pm_batch_tables_current())")
         w("int st = pipeline_%s_batch(n, iparams, fparams, inputs, outputs, "
           "stream);" % name)
         w("if (st) return st;")
         w("if (cudaStreamSynchronize(s) != cudaSuccess) return pm_status = "
           "PM_ERR_CUDA;")
-        w("if (!pm_bgraph_stream && cudaStreamCreateWithFlags("
-          "&pm_bgraph_stream, cudaStreamNonBlocking) != cudaSuccess) return "
-          "pm_status = PM_ERR_CUDA;")
-        w("if (pm_bgraph_exec) { cudaGraphExecDestroy(pm_bgraph_exec); "
-          "pm_bgraph_exec = nullptr; }")
+        w("if (!pm_bgraph_stream[dev] && cudaStreamCreateWithFlags("
+          "&pm_bgraph_stream[dev], cudaStreamNonBlocking) != cudaSuccess) "
+          "return pm_status = PM_ERR_CUDA;")
+        w("if (pm_bgraph_exec[dev]) { cudaGraphExecDestroy("
+          "pm_bgraph_exec[dev]); pm_bgraph_exec[dev] = nullptr; }")
         w("cudaGraph_t g = nullptr;")
-        w("if (cudaStreamBeginCapture(pm_bgraph_stream, "
+        w("if (cudaStreamBeginCapture(pm_bgraph_stream[dev], "
           "cudaStreamCaptureModeThreadLocal) != cudaSuccess) return "
           "pm_status = PM_ERR_CUDA;")
         w("st = pipeline_%s_batch(n, iparams, fparams, inputs, outputs, "
-          "pm_bgraph_stream);   // replays: kernels only" % name)
-        w("cudaError_t e = cudaStreamEndCapture(pm_bgraph_stream, &g);")
+          "pm_bgraph_stream[dev]);   // replays: kernels only" % name)
+        w("cudaError_t e = cudaStreamEndCapture(pm_bgraph_stream[dev], &g);")
         w("if (st || e != cudaSuccess) { if (g) cudaGraphDestroy(g); "
           "cudaGetLastError(); return pm_status = st ? st : PM_ERR_CUDA; }")
-        w("e = cudaGraphInstantiate(&pm_bgraph_exec, g, 0);")
+        w("e = cudaGraphInstantiate(&pm_bgraph_exec[dev], g, 0);")
         w("cudaGraphDestroy(g);")
-        w("if (e != cudaSuccess) { pm_bgraph_exec = nullptr; return "
+        w("if (e != cudaSuccess) { pm_bgraph_exec[dev] = nullptr; return "
           "pm_status = PM_ERR_CUDA; }")
-        w("pm_bgraph_key = key; pm_bgraph_ws = pm_batch_arena.ptr[dev];")
+        w("pm_bgraph_key[dev] = key; pm_bgraph_ws[dev] = "
+          "pm_batch_arena.ptr[dev];")
         w.close()
-        w("if (cudaGraphLaunch(pm_bgraph_exec, s) != cudaSuccess) return "
+        w("if (cudaGraphLaunch(pm_bgraph_exec[dev], s) != cudaSuccess) return "
           "pm_status = PM_ERR_CUDA;")
         w("return pm_status = PM_OK;")
         w.close()
@@ -1612,6 +1671,7 @@ class StencilGen(object):
         w("int first;           // tiles [first, total) of this launch")
         w("int total;           // tiles over all images")
         w("int* queue;          // tile queue counter (persistent launch)")
+        w("int stride;          // no queue: a CTA's tiles are gridDim.x apart")
         w.close("};")
         w("")
         self.gen_kernel()
@@ -1707,6 +1767,11 @@ class StencilGen(object):
         pre = bool(self.stage_nodes) and 'prefetch' in pg.p.options and \
             getattr(plan, 'stage_delta', 0) > 0
         self.prefetch = pre
+        if 'pdl' in pg.p.options:
+            # option 'pdl': launched with programmatic stream serialization;
+            # nothing earlier kernels wrote is read before this wait
+            w("pm_grid_dep_wait();")
+            w("pm_grid_dep_launch();")
         if self.stage_nodes:
             # one mbarrier per copy of the staged inputs, initialized once;
             # each tile that issues TMA loads completes one phase of the
@@ -1737,16 +1802,19 @@ class StencilGen(object):
                 self.gen_wait("pm_bar", "0", None)
             for f in plan.steps:
                 self.gen_step(f)
-            w("if (!L.queue) break;")
+            w("if (!L.queue && !L.stride) break;")
             if self.stage_nodes:
                 w("pm_fence_proxy_async();   // the next tile's TMA rewrites "
                   "smem")
             w("__syncthreads();      // shared memory is reused by the next "
               "tile")
+            w.open("if (L.queue)")
             w("if (threadIdx.x == 0) pm_next_tile = L.first + (int)gridDim.x"
               " + atomicAdd(L.queue, 1);")
             w("__syncthreads();")
             w("tile = pm_next_tile;")
+            w.close()
+            w("else tile += (int)gridDim.x;")
             w.close()
             w.close()
             w("")
@@ -1772,6 +1840,7 @@ class StencilGen(object):
         w("__syncthreads();")
         w("pm_nt = pm_next_tile;")
         w.close()
+        w("else if (L.stride) pm_nt = tile + (int)gridDim.x;")
         w("pm_pend = false;")
         w.open("if (pm_nt < L.total)")
         self.gen_tile_setup("pm_nt")
@@ -2420,13 +2489,23 @@ class StencilGen(object):
             pg.w = self.ctx.w = saved
             self.vec = 1
             self.vec_stats = None
-        return 4 if ok else 1
+        if ok:
+            return 4
+        # 2 points per thread when the stage decides something by the
+        # parity of its innermost index (an upsampling by 2 reading x / 2
+        # and selecting on x % 2): each of the two points then has a known
+        # parity, only the taken arm is evaluated, and both read the same
+        # coarse cells
+        if 'no_vec2' not in pg.p.options and \
+                _inner_parity(f, f.variables[-1]):
+            return 2
+        return 1
 
     def vec_read(self, node, f, args):
         """Text of a 16-byte-vector read covering point ``args`` of smem
         node ``node`` (one lane of a cached float4/int4), or None."""
         ctx = self.ctx
-        if node.func.typ.size() != 4 or not node.in_smem:
+        if node.func.typ.size() != 4 or not node.in_smem or self.vec != 4:
             return None
         res = self.inner_residues()
         if node.func not in res or node._sm_ext[-1] % 4:
@@ -2679,7 +2758,7 @@ class StencilGen(object):
         # index is 4-aligned on interior tiles; base and row strides are
         # checked at run time
         vst = None
-        if V > 1 and n.role == 'out' and n.func is plan.anchor and \
+        if V == 4 and n.role == 'out' and n.func is plan.anchor and \
                 f.typ.size() == 4:
             dlo = _const_int(f.domain[-1].lowerBound)
             if dlo is not None and (self._loop_res[f] - dlo) % 4 == 0:
@@ -2803,7 +2882,20 @@ class StencilGen(object):
         w("return PM_OK;")
         w.close()
         w("")
-        w("static bool %s_attr = false;" % k)
+        w("static bool %s_attr[64];     // per device" % k)
+        w("static int %s_resident[64];  // per device" % k)
+        w("// CTAs of this kernel resident on the current device at once")
+        w.open("static long long %s_resident_now()" % k)
+        w("const int dev = pm_cur_dev();")
+        w.open("if (!%s_resident[dev])" % k)
+        w("int per_sm = 0, sms = 0;")
+        w("cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);")
+        w("cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, %s, %d, %d);"
+          % (k, plan.threads, plan.smem_bytes))
+        w("%s_resident[dev] = (int)pm_llmax(1, (long long)per_sm * sms);" % k)
+        w.close()
+        w("return %s_resident[dev];" % k)
+        w.close()
         w.open("static int launch_%s(pm_args& A, const size_t* wsoff, "
                "cudaStream_t s)" % k)
         w("%s_launch L; memset(&L, 0, sizeof(L));" % k)
@@ -2812,15 +2904,28 @@ class StencilGen(object):
         w("int st = %s(L.d0, A, wsoff, &nt); if (st) return st;" % fill)
         w("if (nt == 0) return PM_OK;")
         w("if (nt > 0x7fffffffLL) return PM_ERR_UNSUPPORTED;")
-        w("L.total = (int)nt; L.queue = nullptr;")
-        w.open("if (!%s_attr)" % k)
+        w("L.total = (int)nt; L.queue = nullptr; L.stride = 0;")
+        w.open("if (!%s_attr[pm_cur_dev()])" % k)
         w("if (cudaFuncSetAttribute(%s, cudaFuncAttributeMaxDynamicShared"
           "MemorySize, %d) != cudaSuccess) return PM_ERR_CUDA;" % (
               k, plan.smem_bytes))
-        w("%s_attr = true;" % k)
+        w("%s_attr[pm_cur_dev()] = true;" % k)
         w.close()
-        w("%s<<<(unsigned)nt, %d, %d, s>>>(L);" % (k, plan.threads,
-                                                  plan.smem_bytes))
+        w("long long grid = nt;")
+        if getattr(self, 'prefetch', False):
+            # prefetching needs several tiles per CTA: as many CTAs as fit
+            # on the GPU at once, each taking every gridDim.x-th tile
+            w.open("if (pm_persistent())")
+            w("const long long res = %s_resident_now();" % k)
+            w("if (nt > res) { grid = res; L.stride = 1; }")
+            w.close()
+        if 'pdl' in pg.p.options:
+            w("if (pm_launch_pdl(%s, (unsigned)grid, %d, %d, s, L) != "
+              "cudaSuccess) return PM_ERR_CUDA;" % (k, plan.threads,
+                                                   plan.smem_bytes))
+        else:
+            w("%s<<<(unsigned)grid, %d, %d, s>>>(L);" % (k, plan.threads,
+                                                        plan.smem_bytes))
         w("return cudaGetLastError() == cudaSuccess ? PM_OK : PM_ERR_CUDA;")
         w.close()
         w("")
@@ -2830,7 +2935,6 @@ class StencilGen(object):
         w("static %s_launch pm_bl_%s;" % (k, k))
         w("static long long pm_bgrid_%s = 0;" % k)
         w("static bool pm_bvalid_%s = false;" % k)
-        w("static int %s_resident = 0;" % k)
         w.open("static int batch_%s(pm_args* As, const size_t* wsoffs, int "
                "nslot, int n, char* pinned, char* ddesc, size_t* doff, "
                "cudaStream_t s, int replay)" % k)
@@ -2862,34 +2966,26 @@ class StencilGen(object):
         w("if (base > 0x7fffffffLL) return PM_ERR_UNSUPPORTED;")
         w("if (cudaMemcpyAsync(ddesc + off, H, sizeof(%s_desc) * n, "
           "cudaMemcpyHostToDevice, s) != cudaSuccess) return PM_ERR_CUDA;" % k)
-        w("cudaEventRecord(pm_batch_event, s);")
+        w("cudaEventRecord(pm_batch_event[pm_cur_dev()], s);")
         w("%s_launch L; memset(&L, 0, sizeof(L));" % k)
         w("L.nimg = n; L.descs = reinterpret_cast<const %s_desc*>(ddesc + "
           "off);" % k)
         w("if (n == 1) L.d0 = H[0];")
         w("L.total = (int)base;")
-        w.open("if (!%s_attr)" % k)
+        w.open("if (!%s_attr[pm_cur_dev()])" % k)
         w("if (cudaFuncSetAttribute(%s, cudaFuncAttributeMaxDynamicShared"
           "MemorySize, %d) != cudaSuccess) return PM_ERR_CUDA;" % (
               k, plan.smem_bytes))
-        w("%s_attr = true;" % k)
+        w("%s_attr[pm_cur_dev()] = true;" % k)
         w.close()
         w("// persistent launch: as many CTAs as fit on the GPU at once; they")
         w("// drain a device-side tile queue spanning every image of the batch")
-        w.open("if (!%s_resident)" % k)
-        w("int per_sm = 0, sms = 0, dev = 0;")
-        w("cudaGetDevice(&dev);")
-        w("cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);")
-        w("cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, %s, %d, %d);"
-          % (k, plan.threads, plan.smem_bytes))
-        w("%s_resident = pm_llmax(1, (long long)per_sm * sms);" % k)
-        w.close()
         w("long long grid = base;")
-        w.open("if (pm_persistent() && base > %s_resident)" % k)
+        w.open("if (pm_persistent() && base > %s_resident_now())" % k)
         w("L.queue = reinterpret_cast<int*>(ddesc + qoff);")
         w("if (cudaMemsetAsync(L.queue, 0, sizeof(int), s) != cudaSuccess) "
           "return PM_ERR_CUDA;")
-        w("grid = %s_resident;" % k)
+        w("grid = %s_resident_now();" % k)
         w.close()
         w("pm_bl_%s = L; pm_bgrid_%s = grid; pm_bvalid_%s = true;" % (k, k, k))
         w("%s<<<(unsigned)grid, %d, %d, s>>>(L);" % (k, plan.threads,
@@ -3194,7 +3290,7 @@ class ReductionGen(object):
         w("return PM_OK;")
         w.close()
         w("")
-        w("static bool %s_attr = false;" % k)
+        w("static bool %s_attr[64];     // per device" % k)
         w.open("static int launch_%s(pm_args& A, const size_t* wsoff, "
                "cudaStream_t s)" % k)
         w("%s_launch L; memset(&L, 0, sizeof(L));" % k)
@@ -3205,11 +3301,11 @@ class ReductionGen(object):
           "255) / 256, 148LL * 16), 256, 0, s>>>(L);" % k)
         w("if (nt == 0) return cudaGetLastError() == cudaSuccess ? PM_OK : "
           "PM_ERR_CUDA;")
-        w.open("if (!%s_attr)" % k)
+        w.open("if (!%s_attr[pm_cur_dev()])" % k)
         w("if (cudaFuncSetAttribute(%s, cudaFuncAttributeMaxDynamicShared"
           "MemorySize, %d) != cudaSuccess) return PM_ERR_CUDA;" % (
               k, max(plan.smem_bytes, 16)))
-        w("%s_attr = true;" % k)
+        w("%s_attr[pm_cur_dev()] = true;" % k)
         w.close()
         w("%s<<<(unsigned)nt, %d, %d, s>>>(L);" % (k, plan.threads,
                                                   max(plan.smem_bytes, 16)))
@@ -3244,7 +3340,7 @@ class ReductionGen(object):
         w("*doff = off + sizeof(%s_desc) * n;" % k)
         w("if (cudaMemcpyAsync(ddesc + off, H, sizeof(%s_desc) * n, "
           "cudaMemcpyHostToDevice, s) != cudaSuccess) return PM_ERR_CUDA;" % k)
-        w("cudaEventRecord(pm_batch_event, s);")
+        w("cudaEventRecord(pm_batch_event[pm_cur_dev()], s);")
         w("%s_launch L; memset(&L, 0, sizeof(L));" % k)
         w("L.nimg = n; L.descs = reinterpret_cast<const %s_desc*>(ddesc + "
           "off);" % k)
@@ -3256,11 +3352,11 @@ class ReductionGen(object):
         w("if (base == 0) return cudaGetLastError() == cudaSuccess ? PM_OK : "
           "PM_ERR_CUDA;")
         w("if (base > 0x7fffffffLL) return PM_ERR_UNSUPPORTED;")
-        w.open("if (!%s_attr)" % k)
+        w.open("if (!%s_attr[pm_cur_dev()])" % k)
         w("if (cudaFuncSetAttribute(%s, cudaFuncAttributeMaxDynamicShared"
           "MemorySize, %d) != cudaSuccess) return PM_ERR_CUDA;" % (
               k, max(plan.smem_bytes, 16)))
-        w("%s_attr = true;" % k)
+        w("%s_attr[pm_cur_dev()] = true;" % k)
         w.close()
         w("%s<<<(unsigned)base, %d, %d, s>>>(L);" % (k, plan.threads,
                                                     max(plan.smem_bytes, 16)))
@@ -3488,7 +3584,7 @@ def generate_code_for_pipeline(pipeline):
     w("")
     w("__device__ unsigned pm_err_word;")
     w("static int pm_status = 0;")
-    w("static cudaEvent_t pm_batch_event = nullptr;")
+    w("static cudaEvent_t pm_batch_event[64];   // per device")
     w("static inline long long pm_nonneg(long long v) { return v < 0 ? 0 : v;"
       " }")
     w("static inline long long pm_llmin(long long a, long long b) { return a "

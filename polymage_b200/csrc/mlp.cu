@@ -203,6 +203,10 @@ int pm_mlp_adam(float* params, const float* grads, float* m, float* v, int D,
 // Concurrency: all calls on one device share the array, so two calls in
 // flight at once (on different streams, or from different host threads
 // without ordering) race on it; issue them on one stream.
+// Device reset: the address is looked up once per device and kept; a
+// cudaDeviceReset unloads this module's device code, after which that
+// address is stale, so a process that resets a device must not call this
+// entry on that device again.
 #include <mutex>
 
 #define PM_MLP_STATIC_FLOATS 196864

@@ -77,6 +77,19 @@ __device__ __forceinline__ void pm_fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+// Programmatic dependent launch: a kernel launched with programmatic
+// stream serialization may start while its predecessor in the stream is
+// still running.  pm_grid_dep_wait() returns once every predecessor grid
+// has completed and its memory is visible (at once when the launch had no
+// such predecessor); pm_grid_dep_launch() lets the next kernel in the
+// stream be scheduled once every CTA of this grid has called it.
+__device__ __forceinline__ void pm_grid_dep_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+__device__ __forceinline__ void pm_grid_dep_launch() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 __device__ __forceinline__ void pm_mbar_arrive_expect_tx(uint64_t* bar,
                                                          uint32_t bytes) {
   asm volatile(
@@ -315,6 +328,37 @@ static int pm_arena_get(pm_arena* a, size_t bytes, void** out) {
 }
 
 static inline size_t pm_align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Launch with programmatic stream serialization (the kernel calls
+// pm_grid_dep_wait before reading what earlier work in the stream wrote).
+template <typename L>
+static cudaError_t pm_launch_pdl(void (*k)(L), unsigned grid, unsigned threads,
+                                 size_t smem, cudaStream_t s, const L& arg) {
+  cudaLaunchConfig_t cfg;
+  memset(&cfg, 0, sizeof(cfg));
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, arg);
+}
+
+// Ordinal of the calling thread's current device, the index of every
+// per-device piece of host state (arenas, streams, graphs, kernel
+// attributes); a process uses devices 0..63.
+static inline int pm_cur_dev() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return 0;
+  }
+  return dev;
+}
 
 // Binary search of a tile index in a batch's tile prefix (descriptors carry
 // their first tile); used by batched launches.

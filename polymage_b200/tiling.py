@@ -408,6 +408,8 @@ def plan_stencil(pipeline, comps):
             role[f] = 'out'
             continue
         mult = _multiplicity(us)
+        if mult > 1 and _disjoint_gather(us, env):
+            mult = 1
         cost = func_cost(f)
         if f.name in forced_smem:
             role[f] = 'smem'
@@ -567,6 +569,46 @@ def _multiplicity(us):
     for m, args in us:
         cnt[id(m)] = cnt.get(id(m), 0) + 1
     return max(cnt.values()) if cnt else 0
+
+
+def _disjoint_gather(us, env):
+    """Whether a producer read at several points per consumer point is
+    still read at most once per point overall: each consumer reads it at
+    tuples that agree, position for position, on distinct plain consumer
+    variables and differ only in integer constants elsewhere (the
+    bilateral grid's ``filtered`` reading ``interpolated(0, x, y)`` and
+    ``interpolated(1, x, y)``), and every consumer variable left out of
+    those positions ranges over one value.  Recomputing such a producer at
+    its reads then costs what storing it would, without the shared-memory
+    round trip."""
+    by = {}
+    for m, args in us:
+        by.setdefault(id(m), (m, []))[1].append(args)
+    for m, tuples in by.values():
+        if len(tuples) < 2:
+            continue
+        used = []
+        for pos in range(len(tuples[0])):
+            col = [Value.numericToValue(t[pos]) for t in tuples]
+            if all(str(c) == str(col[0]) for c in col):
+                v = col[0]
+                if not isinstance(v, C.Variable) or \
+                        isinstance(v, C.Parameter) or \
+                        any(v is u for u in used):
+                    return False
+                used.append(v)
+            elif not all(isinstance(c, Value) and isinstance(c.value, int)
+                         for c in col):
+                return False
+        if len(set(tuple(str(a) for a in t) for t in tuples)) != \
+                len(tuples):
+            return False
+        for v, dom in zip(m.variables, m.domain):
+            if any(v is u for u in used):
+                continue
+            if _const_extent(dom, env) != 1:
+                return False
+    return True
 
 
 def _const_extent(dom, env):
