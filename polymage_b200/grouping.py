@@ -118,6 +118,30 @@ def auto_group(pipeline):
             break
 
 
+def fuse_all(pipeline):
+    """Option 'fuse_all': after the greedy grouping, put every stage that is
+    neither a Reduction nor a const function into one group, when that
+    group has a legal fused-kernel plan (else the greedy result stands).
+    The reference's criterion 5 keeps a DAG like the camera pipe's
+    demosaic (stages read by several siblings) in many groups, each
+    writing its planes to memory and reading them back; one overlapped
+    tile over the whole DAG recomputes halos instead."""
+    groups = [g for g in pipeline.groups
+              if not any(c.is_reduction or c.is_const_func for c in g.comps)]
+    if len(groups) < 2:
+        return
+    merged = []
+    for g in groups:
+        merged += g.comps
+    if not _plan_ok(pipeline, merged):
+        return
+    # merge in an order that keeps every intermediate group convex: the
+    # groups are merged into the first one following the schedule order
+    new = groups[0]
+    for g in groups[1:]:
+        new = pipeline.merge_groups(new, g)
+
+
 def manual_group(pipeline, grouping):
     """User-specified grouping: a list of lists of Functions (the original
     objects passed to buildPipeline).  Functions not listed stay alone, and

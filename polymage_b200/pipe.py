@@ -323,6 +323,8 @@ class Pipeline(object):
             grouping.manual_group(self, self._grouping)
         else:
             grouping.auto_group(self)
+            if 'fuse_all' in self._options:
+                grouping.fuse_all(self)
         schedule.schedule_groups(self)
         for g in self._groups:
             g.plan = tiling.plan_group(self, g)

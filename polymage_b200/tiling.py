@@ -300,12 +300,18 @@ class ConstPlan(object):
 
 
 # ---------------------------------------------------------------------------
-def _tile_sizes_for(pipeline, ndims, anchor=None, env=None):
+def _tile_sizes_for(pipeline, ndims, anchor=None, env=None, funcs=()):
     """Tile extent per anchor dimension: the tile sizes apply to the
     innermost dimensions, leading ones get 1.  With fewer sizes than
     dimensions, an innermost dimension of constant extent <= 4 (the
     channels of an interleaved image, [x][y][c]) is tiled whole and the
-    sizes go to the dimensions before it."""
+    sizes go to the dimensions before it.  A leading dimension of constant
+    extent <= 4 (the channels of a planar image, [c][x][y]) can also be
+    tiled whole when the group computes stages of fewer dimensions than the
+    anchor (the camera pipe's red, green and blue planes feeding every
+    output channel): one tile then computes them once for all channels
+    instead of once per channel (option 'channel_tile'; measured slower
+    on the camera pipe, 0.207 vs 0.190 ms, and the pyramids)."""
     ts = list(pipeline.tile_sizes)
     opt = _option(pipeline, 'tile')
     if opt is not None:
@@ -319,7 +325,14 @@ def _tile_sizes_for(pipeline, ndims, anchor=None, env=None):
             tail = [int(e)]
     n = ndims - len(tail)
     head = [int(t) for t in ts[max(0, len(ts) - n):]]
-    return [1] * (n - len(head)) + head + tail
+    lead = [1] * (n - len(head))
+    if lead and not tail and env is not None and \
+            'channel_tile' in pipeline.options and \
+            any(f.ndims < ndims for f in funcs if f is not anchor):
+        e = _const_extent(anchor.domain[0], env)
+        if e is not None and e <= 4:
+            lead[0] = int(e)
+    return lead + head + tail
 
 
 def _option(pipeline, name, default=None):
@@ -385,7 +398,7 @@ def plan_stencil(pipeline, comps):
     plan.threads = int(_option(pipeline, 'threads', DEFAULT_THREADS))
     budget = int(_option(pipeline, 'inline_budget', DEFAULT_INLINE_BUDGET))
     forced_smem = set(_option(pipeline, 'materialize', []) or [])
-    plan.tile = _tile_sizes_for(pipeline, anchor.ndims, anchor, env)
+    plan.tile = _tile_sizes_for(pipeline, anchor.ndims, anchor, env, funcs)
 
     # ---- materialization decisions, sinks first --------------------------
     uses = {}          # func -> [(M func, [arg exprs])]

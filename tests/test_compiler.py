@@ -224,14 +224,20 @@ def _tile_boxes(plan, env):
 @pytest.mark.parametrize("name,sizes", [
     ("pyramid8", (256, 300)), ("pyramid8", (37, 53)),
     ("pyramid", (157, 211)), ("campipe", (200, 264)),
-    ("laplacian", (64 + 92, 96 + 92)), ("bilateral", (77, 93))])
+    ("laplacian", (64 + 92, 96 + 92)), ("bilateral", (77, 93)),
+    ("campipe+fuse_all", (200, 264)), ("campipe+fuse_all", (131, 197))])
 def test_static_extents_cover_every_tile_of_every_group(name, sizes):
     """Region inference for every tile of every fused group of a shipped
     pipeline at a small size: each materialized node's region fits the
     static shared-memory extents the kernel was generated with (a region
-    larger than its buffer would read or write out of it)."""
+    larger than its buffer would read or write out of it).  ``+opt``
+    adds a build option to the catalog's."""
     from polymage_b200.apps import catalog
+    name, _, extra = name.partition('+')
     b, kw = catalog._BUILDERS[name]
+    kw = dict(kw)
+    if extra:
+        kw['options'] = tuple(kw.get('options', ())) + (extra,)
     p = b(**kw)
     env = p.int_env()
     for k in list(env):

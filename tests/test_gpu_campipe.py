@@ -78,3 +78,22 @@ def test_campipe_matches_reference_spec_fixtures(cp):
                     {'img': img, 'matrix_3200': OC.MATRIX_3200,
                      'matrix_7000': OC.MATRIX_7000}, {'process': out})
         assert np.array_equal(out, z['out%d' % n])
+
+
+@pytest.mark.parametrize("R,C", [(1968, 2592), (131, 197), (80, 120)])
+def test_campipe_fused_into_one_group_bit_exact(R, C):
+    """Option 'fuse_all': every non-const stage in one overlapped-tile
+    kernel (one group instead of the greedy grouping's six)."""
+    b, kw = catalog._BUILDERS["campipe"]
+    kw = dict(kw)
+    kw['options'] = tuple(kw['options']) + ('fuse_all',)
+    cp = b(**kw).build()
+    assert sum(1 for g in cp.module.meta['groups']
+               if g['kind'] == 'stencil') == 1
+    img = OC.make_input(R, C, seed=R * 3 + C)
+    out = np.zeros((3, R - 48, C - 64), np.uint8)
+    cp.run_host({'C': C, 'R': R, 'colour_temp': 3700.0, 'contrast': 50.0,
+                 'gamma': 2.0}, {'img': img, 'matrix_3200': OC.MATRIX_3200,
+                                 'matrix_7000': OC.MATRIX_7000},
+                {'process': out})
+    assert np.array_equal(out, OC.campipe(img, 3700.0, 50.0, 2.0))
