@@ -114,6 +114,11 @@ def expected(app, params, inputs):
                 'vcycle3d': 'Vcycle3d', 'wcycle3d': 'Wcycle3d'}[app]
         return {name: fn(inputs['V_'], inputs['F_'], params['n'], **kw)}, \
             {name: None}
+    if app == 'nlmeans':
+        from . import nlmeans as ONL
+        return ({'non_local_means': ONL.nlmeans(
+            inputs['img'], params['patch_size'], params['search_area'])},
+            {'non_local_means': None})
     if app == 'mg3p':
         from polymage_b200.apps import catalog
         u, r = ON.mg3p(inputs['U'], inputs['V'], inputs['R'],

@@ -29,6 +29,7 @@ from .interpolate import build_interpolate
 from .jacobi import build_jacobi2d, build_jacobi3d
 from .multigrid import build_v_cycle
 from .nas_mg import build_mg3p
+from .nlmeans import build_nlmeans
 
 HARRIS = dict(tile_sizes=(16, 128), group_size=11,
               options=('rblock=8', 'min_blocks=4'))
@@ -63,6 +64,9 @@ VCYCLE3D = dict(n=31, L=3, nu1=10, nu2=0, nuc=0, dims=3,
                 tile_sizes=(4, 8, 32), group_size=4, name="Vcycle3d")
 WCYCLE3D = dict(VCYCLE3D, gamma=2, name="Wcycle3d")
 MG3P = dict(prob_class='W', tile_sizes=(4, 8, 32), group_size=6)
+# non-local means at the reference Makefile's patch size and search area
+# (non_local_means/Makefile:11-12) on a 256x256 image
+NLMEANS = dict(rows=256, cols=256)
 
 _BUILDERS = {
     "harris": (build_harris, HARRIS),
@@ -80,6 +84,7 @@ _BUILDERS = {
     "vcycle3d": (build_v_cycle, VCYCLE3D),
     "wcycle3d": (build_v_cycle, WCYCLE3D),
     "mg3p": (build_mg3p, MG3P),
+    "nlmeans": (build_nlmeans, NLMEANS),
 }
 
 _cache = {}

@@ -27,7 +27,7 @@ APPS = ("harris", "unsharp", "campipe", "bilateral", "pyramid", "pyramid8",
 # Makefiles' sizes (catalog); for the grids "pixels" are the interior
 # points a call updates
 WIDENING = ("interpolate", "jacobi2d", "jacobi3d", "vcycle", "wcycle",
-            "vcycle3d", "wcycle3d", "mg3p")
+            "vcycle3d", "wcycle3d", "mg3p", "nlmeans")
 FLUSH_BYTES = 256 << 20
 
 
@@ -126,6 +126,18 @@ def workload(app, seed=0):
                 {'MG_U': (shape, np.float64), 'MG_R': (shape, np.float64)},
                 n ** 3, "NAS MG mg3P class %s (%d^3) float64"
                 % (catalog.MG3P['prob_class'], n))
+    if app == 'nlmeans':
+        R, C = catalog.NLMEANS['rows'], catalog.NLMEANS['cols']
+        x = np.arange(R)[:, None] / R
+        y = np.arange(C)[None, :] / C
+        img = np.empty((3, R, C), np.float32)
+        for c in range(3):
+            img[c] = 0.5 + 0.3 * np.sin(6.0 * x + 2.0 * c) * \
+                np.cos(5.0 * y) + 0.02 * rng.standard_normal((R, C))
+        return ({'R': R, 'C': C, 'patch_size': 7, 'search_area': 7},
+                {'img': img}, {'non_local_means': ((3, R, C), np.float32)},
+                R * C, "non_local_means %dx%d RGB float32, patch 7, search "
+                "area 7" % (R, C))
     raise ValueError(app)
 
 

@@ -284,9 +284,18 @@ def restrict_range(lo, hi, k, r):
 
 def bounds_check_pass(pipeline):
     """Check every reference of every compute object at the parameter
-    estimates; record the symbolic checks for the run-time validator."""
+    estimates; record the symbolic checks for the run-time validator.
+
+    With option 'oob_zero' a read of an input image outside its domain is
+    not refused: the image and dimension are recorded in
+    ``pipeline._oob_dims`` ({Image: set of dims}) and the generated code
+    reads 0 there (the convention of points nothing defines); such reads
+    get no run-time check.  Reads of computed stages must stay inside
+    their domains either way."""
     env = pipeline.int_env()
     checks = []
+    oob_zero = 'oob_zero' in pipeline.options
+    pipeline._oob_dims = {}
     for comp in pipeline.comps:
         f = comp.func
         for box, cond, expr, red in part_boxes(f):
@@ -317,10 +326,14 @@ def bounds_check_pass(pipeline):
                     r = expr_range(arg, rr, env)
                     if r is None:
                         continue
-                    checks.append((comp, box, arg, g, dim, is_target,
-                                   restr))
                     dlo = eval_int(dom.lowerBound, env)
                     dhi = eval_int(dom.upperBound, env)
+                    if oob_zero and isinstance(g, C.Image) and \
+                            not is_target and (r[0] < dlo or r[1] > dhi):
+                        pipeline._oob_dims.setdefault(g, set()).add(dim)
+                        continue
+                    checks.append((comp, box, arg, g, dim, is_target,
+                                   restr))
                     if r[0] < dlo or r[1] > dhi:
                         LOG.error("Reference out of domain: %s in %s, dim %d"
                                   " referenced [%d, %d], domain [%d, %d]",

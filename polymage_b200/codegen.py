@@ -703,6 +703,24 @@ class PipelineGen(object):
                     s, n, d, n, d))
         return " + ".join(terms)
 
+    def oob_guard(self, f, args, ctx):
+        """Under option 'oob_zero': the C condition that a read of input
+        image ``f`` at ``args`` lies inside its domain along the dimensions
+        the bounds check found it can leave (None when no guard is
+        needed); the read yields 0 where the condition fails."""
+        dims = getattr(self.p, '_oob_dims', {}).get(f)
+        if not dims:
+            return None
+        n = self.fn(f)
+        conds = []
+        for d in sorted(dims):
+            a = args[d]
+            t = ctx.index(a) if not is_data_dependent(a) else \
+                ctx.expr(a, {})
+            conds.append("(%s) >= d_%s_lo%d && (%s) <= d_%s_hi%d" % (
+                t, n, d, t, n, d))
+        return " && ".join(conds)
+
     def host_text(self):
         if not self.hw.lines:
             return None
@@ -2218,6 +2236,21 @@ class StencilGen(object):
         w = pg.w
         node = plan.node_of.get(f)
         t = ctx.temp()
+        guard = pg.oob_guard(f, args, ctx)
+        if guard is not None:
+            # reads outside the image's domain yield 0 (option 'oob_zero')
+            if node is not None and node.in_smem:
+                idx = self.smem_index(node, args)
+                w("const %s %s = (%s) ? sm_%s[%s] : (%s)0;" % (
+                    ctype(f.typ), t, guard, self.node_name(node), idx,
+                    ctype(f.typ)))
+            else:
+                w("const %s %s = (%s) ? __ldg(b_%s + (%s)) : (%s)0;" % (
+                    ctype(f.typ), t, guard, pg.fn(f),
+                    pg.gindex(f, args, ctx, clamp_all=self.clamp),
+                    ctype(f.typ)))
+            ctx.define(key, t)
+            return t
         if node is not None and node.in_smem and self.vec > 1 and \
                 self.inside:
             vt = self.vec_read(node, f, args)
@@ -3249,8 +3282,15 @@ class ReductionGen(object):
         if hit is not None:
             return hit
         t = ctx.temp()
-        pg.w("const %s %s = __ldg(b_%s + (%s));" % (
-            ctype(f.typ), t, pg.fn(f), pg.gindex(f, args, ctx)))
+        guard = pg.oob_guard(f, args, ctx)
+        if guard is not None:
+            # reads outside the image's domain yield 0 (option 'oob_zero')
+            pg.w("const %s %s = (%s) ? __ldg(b_%s + (%s)) : (%s)0;" % (
+                ctype(f.typ), t, guard, pg.fn(f), pg.gindex(f, args, ctx),
+                ctype(f.typ)))
+        else:
+            pg.w("const %s %s = __ldg(b_%s + (%s));" % (
+                ctype(f.typ), t, pg.fn(f), pg.gindex(f, args, ctx)))
         ctx.define(key, t)
         return t
 

@@ -23,17 +23,23 @@ _INTS = (C.Int, C.UInt, C.Short, C.UShort, C.Char, C.UChar, C.Long,
 
 
 class Evaluator(object):
-    def __init__(self, params, images):
+    def __init__(self, params, images, oob_zero=False):
         """``params``: {name: value}; ``images``: {name: numpy array}
-        indexed from 0 (the image's domain lower bounds are 0)."""
+        indexed from 0 (the image's domain lower bounds are 0).
+        ``oob_zero``: an image read outside the array reads 0 (the
+        convention of compiler option 'oob_zero')."""
         self.params = params
         self.images = images
+        self.oob_zero = oob_zero
         self.memo = {}
 
     def value(self, f, args):
         args = tuple(int(a) for a in args)
         if isinstance(f, C.Image):
             a = self.images[f.name]
+            if self.oob_zero and any(i < 0 or i >= n
+                                     for i, n in zip(args, a.shape)):
+                return 0.0
             return a[args].item()
         key = (id(f), args)
         if key in self.memo:
@@ -121,7 +127,12 @@ class Evaluator(object):
             if op == '*':
                 return a * b
             if op == '/':
-                return c_div(a, b) if ints else a / b
+                if ints:
+                    return c_div(a, b)
+                if b == 0:                  # IEEE: 0/0 is NaN, x/0 inf
+                    return float('nan') if a == 0 or a != a else \
+                        math.copysign(math.inf, a) * math.copysign(1.0, b)
+                return a / b
             if op == '%':
                 return c_mod(a, b)
             raise NotImplementedError(op)

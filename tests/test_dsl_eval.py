@@ -162,3 +162,15 @@ def test_nas_mg_restatement_matches_statement():
         ou, orr = ON.mg3p(U, V, R, 'S')
         assert np.abs(ev.array(u) - ou).max() <= 1e-12
         assert np.abs(ev.array(r) - orr).max() <= 1e-12
+
+
+def test_nlmeans_restatement_matches_statement():
+    """Non-local means (image channel 3 read as 0, option 'oob_zero')."""
+    import oracle.nlmeans as ONL
+    from polymage_b200.apps.nlmeans import nlmeans
+    R, C, p, s = 13, 15, 3, 3
+    img = ONL.make_input(R, C, seed=1)
+    ev = Evaluator({'R': R, 'C': C, 'patch_size': p, 'search_area': s},
+                   {'img': img.astype(np.float64)}, oob_zero=True)
+    got = ev.array(nlmeans({}))
+    assert np.abs(got - ONL.nlmeans(img, p, s)).max() <= 1e-12
