@@ -114,6 +114,9 @@ def expected(app, params, inputs):
                 'vcycle3d': 'Vcycle3d', 'wcycle3d': 'Wcycle3d'}[app]
         return {name: fn(inputs['V_'], inputs['F_'], params['n'], **kw)}, \
             {name: None}
+    if app == 'maxfilter':
+        from . import maxfilter as OMF
+        return {'final': OMF.maxfilter(inputs['img'])}, {'final': None}
     if app == 'nlmeans':
         from . import nlmeans as ONL
         return ({'non_local_means': ONL.nlmeans(

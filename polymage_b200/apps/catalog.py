@@ -8,8 +8,9 @@ and faster than their best (0.029 vs 0.034 ms).  Unsharp recomputes blurx
 inside blury (a larger inline budget) on 128x128 tiles, also outside the
 tuned space: with 16-byte shared-memory reads the recomputation is cheaper
 than a second shared-memory stage and its barrier (0.087-0.090 vs
-0.094 ms for the tuned best).  The camera pipe fuses with group size 12
-(one group more than the tuned best at 9: 0.197 vs 0.211 ms).  Harris,
+0.094 ms for the tuned best).  The camera pipe fuses every stage into one
+group (option fuse_all; the greedy grouping leaves six kernels: 0.133 vs
+0.190 ms) on 64x128 tiles.  Harris,
 the camera pipe and both pyramids ask ptxas for 4 resident CTAs per SM
 (``min_blocks=4``: at most 64 registers a thread), also outside the tuned
 space: 0.0290 vs 0.0303 ms, 0.185 vs 0.195 ms, 0.203 vs 0.209 ms and
@@ -30,13 +31,14 @@ from .jacobi import build_jacobi2d, build_jacobi3d
 from .multigrid import build_v_cycle
 from .nas_mg import build_mg3p
 from .nlmeans import build_nlmeans
+from .max_filter import build_maxfilter
 
 HARRIS = dict(tile_sizes=(16, 128), group_size=11,
               options=('rblock=8', 'min_blocks=4'))
 UNSHARP = dict(tile_sizes=(128, 128), group_size=10,
                options=('rblock=8', 'inline_budget=400'))
-CAMPIPE = dict(tile_sizes=(32, 64), group_size=12,
-               options=('rblock=8', 'min_blocks=4'))
+CAMPIPE = dict(tile_sizes=(64, 128), group_size=12,
+               options=('rblock=8', 'min_blocks=4', 'fuse_all'))
 BILATERAL = dict(tile_sizes=(1, 32, 128), group_size=10,
                  options=(('red_tile', (32, 256)), 'rblock=4'))
 PYRAMID = dict(tile_sizes=(32, 64), group_size=10,
@@ -67,6 +69,9 @@ MG3P = dict(prob_class='W', tile_sizes=(4, 8, 32), group_size=6)
 # non-local means at the reference Makefile's patch size and search area
 # (non_local_means/Makefile:11-12) on a 256x256 image
 NLMEANS = dict(rows=256, cols=256)
+# max filter (radius 26) on a 1536x2560 landscape image: the spec's
+# vert_log rows are [26, C-R-79], non-empty only when C > R + 104
+MAXFILTER = dict(rows=1536, cols=2560)
 
 _BUILDERS = {
     "harris": (build_harris, HARRIS),
@@ -85,6 +90,7 @@ _BUILDERS = {
     "wcycle3d": (build_v_cycle, WCYCLE3D),
     "mg3p": (build_mg3p, MG3P),
     "nlmeans": (build_nlmeans, NLMEANS),
+    "maxfilter": (build_maxfilter, MAXFILTER),
 }
 
 _cache = {}

@@ -27,7 +27,7 @@ APPS = ("harris", "unsharp", "campipe", "bilateral", "pyramid", "pyramid8",
 # Makefiles' sizes (catalog); for the grids "pixels" are the interior
 # points a call updates
 WIDENING = ("interpolate", "jacobi2d", "jacobi3d", "vcycle", "wcycle",
-            "vcycle3d", "wcycle3d", "mg3p", "nlmeans")
+            "vcycle3d", "wcycle3d", "mg3p", "nlmeans", "maxfilter")
 FLUSH_BYTES = 256 << 20
 
 
@@ -126,6 +126,13 @@ def workload(app, seed=0):
                 {'MG_U': (shape, np.float64), 'MG_R': (shape, np.float64)},
                 n ** 3, "NAS MG mg3P class %s (%d^3) float64"
                 % (catalog.MG3P['prob_class'], n))
+    if app == 'maxfilter':
+        R, C = catalog.MAXFILTER['rows'], catalog.MAXFILTER['cols']
+        return ({'R': R, 'C': C},
+                {'img': rng.integers(0, 256, (3, R, C)).astype(np.float32)},
+                {'final': ((R, C, 3), np.int32)}, R * C,
+                "max_filter %dx%d RGB (0..255 as float32), radius 26" % (
+                    R, C))
     if app == 'nlmeans':
         R, C = catalog.NLMEANS['rows'], catalog.NLMEANS['cols']
         x = np.arange(R)[:, None] / R

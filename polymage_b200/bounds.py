@@ -286,12 +286,11 @@ def bounds_check_pass(pipeline):
     """Check every reference of every compute object at the parameter
     estimates; record the symbolic checks for the run-time validator.
 
-    With option 'oob_zero' a read of an input image outside its domain is
-    not refused: the image and dimension are recorded in
-    ``pipeline._oob_dims`` ({Image: set of dims}) and the generated code
-    reads 0 there (the convention of points nothing defines); such reads
-    get no run-time check.  Reads of computed stages must stay inside
-    their domains either way."""
+    With option 'oob_zero' a read outside the producer's domain is not
+    refused: the producer and dimension are recorded in
+    ``pipeline._oob_dims`` ({producer: set of dims}) and the generated
+    code reads 0 there (the convention of points nothing defines); such
+    reads get no run-time check."""
     env = pipeline.int_env()
     checks = []
     oob_zero = 'oob_zero' in pipeline.options
@@ -328,8 +327,8 @@ def bounds_check_pass(pipeline):
                         continue
                     dlo = eval_int(dom.lowerBound, env)
                     dhi = eval_int(dom.upperBound, env)
-                    if oob_zero and isinstance(g, C.Image) and \
-                            not is_target and (r[0] < dlo or r[1] > dhi):
+                    if oob_zero and not is_target and \
+                            (r[0] < dlo or r[1] > dhi):
                         pipeline._oob_dims.setdefault(g, set()).add(dim)
                         continue
                     checks.append((comp, box, arg, g, dim, is_target,

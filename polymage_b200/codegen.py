@@ -704,10 +704,10 @@ class PipelineGen(object):
         return " + ".join(terms)
 
     def oob_guard(self, f, args, ctx):
-        """Under option 'oob_zero': the C condition that a read of input
-        image ``f`` at ``args`` lies inside its domain along the dimensions
-        the bounds check found it can leave (None when no guard is
-        needed); the read yields 0 where the condition fails."""
+        """Under option 'oob_zero': the C condition that a read of ``f``
+        at ``args`` lies inside its domain along the dimensions the bounds
+        check found it can leave (None when no guard is needed); the read
+        yields 0 where the condition fails."""
         dims = getattr(self.p, '_oob_dims', {}).get(f)
         if not dims:
             return None
@@ -2244,6 +2244,10 @@ class StencilGen(object):
                 w("const %s %s = (%s) ? sm_%s[%s] : (%s)0;" % (
                     ctype(f.typ), t, guard, self.node_name(node), idx,
                     ctype(f.typ)))
+            elif f in plan.role and plan.role[f] == 'inline':
+                raise CodegenError("option oob_zero: %s is read outside "
+                                   "its domain and computed inline; it "
+                                   "must be materialized" % f.name)
             else:
                 w("const %s %s = (%s) ? __ldg(b_%s + (%s)) : (%s)0;" % (
                     ctype(f.typ), t, guard, pg.fn(f),
@@ -3181,10 +3185,15 @@ class ReductionGen(object):
             w("for (int i = threadIdx.x; i < %d; i += %d) acc[i] = %s;" % (
                 ptot, plan.threads, ident))
             w("__syncthreads();")
-        # loop over the tile's reduction points
+        # loop over the tile's reduction points; unrolled (option
+        # 'red_unroll', default 4) so that the loads of several points are
+        # in flight before their atomics
         tot = 1
         for t in plan.tile:
             tot *= t
+        un = int(_opt(pg.p, 'red_unroll', 4) or 1)
+        if un > 1:
+            w("#pragma unroll %d" % un)
         w.open("for (int i = threadIdx.x; i < %d; i += %d)" % (tot,
                                                                plan.threads))
         StencilGen.decompose(self, "i", plan.tile, "j")

@@ -166,7 +166,7 @@ def monotone_dir(expr, var):
     if isinstance(expr, C.Parameter):
         return 0
     if isinstance(expr, C.Variable):
-        return 1 if expr is var else None
+        return 1 if expr is var else 0      # another variable is held fixed
     if isinstance(expr, AbstractUnaryOpNode):
         d = monotone_dir(expr.child, var)
         if d is None:

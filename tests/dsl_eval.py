@@ -113,8 +113,17 @@ class Evaluator(object):
         if isinstance(e, C.Variable):
             return env[id(e)]
         if isinstance(e, C.Reference):
-            return self.value(e.objectRef, [self.expr(a, env)
-                                            for a in e.arguments])
+            f = e.objectRef
+            args = [self.expr(a, env) for a in e.arguments]
+            if not isinstance(f, C.Image):
+                # a data-dependent index is clamped into the producer's
+                # domain, as the compiled code clamps it
+                for d, a in enumerate(e.arguments):
+                    if a.has(C.Reference) if hasattr(a, 'has') else False:
+                        lo = self.expr(f.domain[d].lowerBound, {})
+                        hi = self.expr(f.domain[d].upperBound, {})
+                        args[d] = min(max(args[d], lo), hi)
+            return self.value(f, args)
         if isinstance(e, AbstractBinaryOpNode):
             a = self.expr(e.left, env)
             b = self.expr(e.right, env)

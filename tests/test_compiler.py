@@ -347,6 +347,8 @@ def _next_app(name):
         sizes = {key: int(size)}
         if app in ("interpolate", "nlmeans"):
             sizes = {'R': int(size), 'C': int(size) * 3 // 4 + 1}
+        if app == "maxfilter":
+            sizes = {'R': int(size), 'C': int(size) * 3}
         return b(**kw), sizes
     from polymage_b200.apps.nas_mg import build_mg3p
     return build_mg3p('S'), {'n': 32}
@@ -357,7 +359,7 @@ def _next_app(name):
     "catalog:interpolate@211", "catalog:jacobi2d@333",
     "catalog:jacobi3d@47", "catalog:vcycle@20", "catalog:wcycle@13",
     "catalog:vcycle3d@8", "catalog:wcycle3d@6", "catalog:mg3p@128",
-    "catalog:nlmeans@37"])
+    "catalog:nlmeans@37", "catalog:maxfilter@90"])
 def test_static_extents_cover_every_tile_next_apps(name):
     """The same tile-by-tile check for the widening apps, at sizes their
     GPU tests run."""

@@ -174,3 +174,17 @@ def test_nlmeans_restatement_matches_statement():
                    {'img': img.astype(np.float64)}, oob_zero=True)
     got = ev.array(nlmeans({}))
     assert np.abs(got - ONL.nlmeans(img, p, s)).max() <= 1e-12
+
+
+def test_maxfilter_restatement_matches_statement():
+    """Max filter (vert_log read as 0 outside its domain, option
+    'oob_zero'; data-dependent slice indices clamped)."""
+    import oracle.maxfilter as OMF
+    from polymage_b200.apps.max_filter import maxfilter
+    R, C = 84, 196
+    img = OMF.make_input(R, C, seed=2)
+    ev = Evaluator({'R': R, 'C': C}, {'img': img.astype(np.float64)},
+                   oob_zero=True)
+    got = ev.array(maxfilter({}))
+    ref = OMF.maxfilter(img)
+    assert (ref > 0).any() and np.array_equal(got, ref)
