@@ -5,10 +5,15 @@ timed runs each with L2 flushed; polymage_b200.autotune).  Harris keeps the
 group size of the reference's Harris builder (11: all stages in one group,
 harris/builder.py:66-67), which is outside the tuned group sizes (3..10)
 and faster than their best (0.029 vs 0.034 ms).  Unsharp recomputes blurx
-inside blury (a larger inline budget) on 128x128 tiles, also outside the
-tuned space: with 16-byte shared-memory reads the recomputation is cheaper
-than a second shared-memory stage and its barrier (0.087-0.090 vs
-0.094 ms for the tuned best).  The camera pipe fuses every stage into one
+inside blury (a larger inline budget), also outside the tuned space: with
+16-byte shared-memory reads the recomputation is cheaper than a second
+shared-memory stage and its barrier (0.087-0.090 vs 0.094 ms for the
+tuned best); CTAs of 128 threads on 64x128 tiles with 16 rows per thread
+keep more, smaller CTAs resident (0.0773 vs 0.0866 ms with 256 threads).
+Harris also runs 128-thread CTAs, on 32x64 tiles (0.0273 vs 0.0291 ms).
+The bilateral grid's construction takes 16x256-pixel tiles (0.0908 vs
+0.1033 ms with 32x256), interpolation 32x64 tiles (0.53 vs 1.69 ms with
+the reference builder's 16x16).  The camera pipe fuses every stage into one
 group (option fuse_all; the greedy grouping leaves six kernels: 0.133 vs
 0.190 ms) on 64x128 tiles.  Harris,
 the camera pipe and both pyramids ask ptxas for 4 resident CTAs per SM
@@ -33,14 +38,14 @@ from .nas_mg import build_mg3p
 from .nlmeans import build_nlmeans
 from .max_filter import build_maxfilter
 
-HARRIS = dict(tile_sizes=(16, 128), group_size=11,
-              options=('rblock=8', 'min_blocks=4'))
-UNSHARP = dict(tile_sizes=(128, 128), group_size=10,
-               options=('rblock=8', 'inline_budget=400'))
+HARRIS = dict(tile_sizes=(32, 64), group_size=11,
+              options=('rblock=8', 'min_blocks=4', 'threads=128'))
+UNSHARP = dict(tile_sizes=(64, 128), group_size=10,
+               options=('rblock=16', 'inline_budget=400', 'threads=128'))
 CAMPIPE = dict(tile_sizes=(64, 128), group_size=12,
                options=('rblock=8', 'min_blocks=4', 'fuse_all'))
 BILATERAL = dict(tile_sizes=(1, 32, 128), group_size=10,
-                 options=(('red_tile', (32, 256)), 'rblock=4'))
+                 options=(('red_tile', (16, 256)), 'rblock=4'))
 PYRAMID = dict(tile_sizes=(32, 64), group_size=10,
                options=('rblock=8', 'min_blocks=4'))
 # 8 levels, indices clamped at every level's borders (any image size)
@@ -56,7 +61,7 @@ LAPLACIAN = dict(tile_sizes=(32, 64), group_size=10, options=('rblock=8',))
 # grid, 10 pre-smoothings and none after or on the coarsest level
 # (multigrid/jacobi{2D,3D}/Makefile:10-16), NAS MG class W (NAS-PB-MG-3.2/
 # Makefile:9), interpolation of a 2048x2048 RGBA image.
-INTERPOLATE = dict(rows=2048, cols=2048, tile_sizes=(16, 16), group_size=11)
+INTERPOLATE = dict(rows=2048, cols=2048, tile_sizes=(32, 64), group_size=11)
 JACOBI2D = dict(N=2048, T=10, tile_sizes=(16, 64), group_size=10)
 JACOBI3D = dict(N=128, T=10, tile_sizes=(4, 8, 32), group_size=5)
 VCYCLE = dict(n=31, L=3, nu1=10, nu2=0, nuc=0, tile_sizes=(16, 64),

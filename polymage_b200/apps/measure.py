@@ -217,6 +217,46 @@ def measure(app, steps=50, warmup=5, device=None, graph=True, warm=False,
                    "256 MB written before each timed run")}
 
 
+def int_peak(device=None, iters=4096, steps=20):
+    """Integer-ALU throughput of the GPU (thread instructions per second)
+    from polymage_b200/csrc/int_peak.cu: 8 independent 32-bit
+    multiply-add chains (IMAD) or add/xor chains per thread, 148 x 16
+    CTAs of 256 threads, CUDA events, best of ``steps`` runs.  Each round
+    of the IMAD kernel is 8 integer instructions per thread and of the ALU
+    kernel 18 (8 adds, 8 xors, and the two updates of its operands)."""
+    import ctypes
+    import torch
+    from ..build import compile_source
+    here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    lib = ctypes.CDLL(compile_source("int_peak", os.path.join(
+        here, "csrc", "int_peak.cu")))
+    lib.pm_int_peak_run.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p,
+                                                         ctypes.c_void_p]
+    dev = device or torch.device("cuda", torch.cuda.current_device())
+    blocks = 148 * 16
+    out = torch.empty(blocks * 256, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    res = {}
+    for which, name, per_round in ((0, "imad", 8), (1, "add_xor", 18)):
+        best = None
+        for i in range(steps + 2):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            if lib.pm_int_peak_run(which, blocks, iters, out.data_ptr(),
+                                   stream.cuda_stream) != 0:
+                raise RuntimeError("int_peak launch failed")
+            b.record(stream)
+            torch.cuda.synchronize(dev)
+            if i >= 2:
+                ms = a.elapsed_time(b)
+                best = ms if best is None else min(best, ms)
+        n = float(blocks) * 256 * iters * per_round
+        res[name] = {"ms": best, "thread_inst_per_s": n / (best / 1e3),
+                     "thread_inst_per_launch": n}
+    return res
+
+
 def measure_host(app, steps=10, warmup=2):
     """End to end through the reference's C ABI (``pipeline_<name>`` on
     pinned host buffers: copies to and from the device inside the call),
@@ -335,7 +375,12 @@ def main():
                     help="no L2 flush between runs (single-image pipelines)")
     ap.add_argument("--host", action="store_true",
                     help="end to end through the host-buffer C ABI")
+    ap.add_argument("--int-peak", action="store_true",
+                    help="integer-ALU throughput of the GPU")
     args = ap.parse_args()
+    if args.int_peak:
+        print(json.dumps(int_peak()))
+        return
     for app in args.app or APPS + ("bilateral_batch64", "stream1024"):
         if app == "stream1024":
             print(json.dumps(measure_stream(1024)))

@@ -3223,8 +3223,12 @@ class ReductionGen(object):
             cn = ["c%d_%d" % (d, pi) for d in range(nd)]
             for d, ta in enumerate(tgt):
                 w("const int %s = %s;" % (cn[d], ctx.expr(ta, rbind)))
+            # target coordinates that do not depend on data are inside
+            # the domain wherever the call passed the bounds validation;
+            # only data-dependent ones (a bin index) are tested
             inb = " && ".join("%s >= d_%s_lo%d && %s <= d_%s_hi%d" % (
-                cn[d], fnm, d, cn[d], fnm, d) for d in range(nd))
+                cn[d], fnm, d, cn[d], fnm, d) for d in range(nd)
+                if is_data_dependent(tgt[d])) or "true"
             cc = ctx.cond(cond, tbind) if cond is not None else "true"
             val = ctx.expr(expr, rbind) if shared else None
             w.open("if ((%s) && (%s))" % (inb, cc))
