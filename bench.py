@@ -203,6 +203,44 @@ def pipeline_check(app, dev):
     return {"error": err, "cpu_baseline": base}
 
 
+def learned_vs_exhaustive():
+    """The learned tuner replayed on the committed B200 timing database
+    (polymage_b200/data/timing_db_b200.jsonl: every configuration of the
+    reference's search space, measured): per pipeline, the cost model is
+    trained on the GPU by this package's kernels on the other pipelines'
+    rows only, picks 14 configurations, and its best pick's time is
+    compared with the database's best (the exhaustive result)."""
+    from polymage_b200 import costmodel, tuner
+    rows = tuner.load_db(costmodel.DB_PATH)
+    out = {}
+    for app in sorted(set(r['app'] for r in rows)):
+        t0 = time.time()
+        ratio, n, uniq = costmodel.evaluate_on_db(rows, app, seed=0)
+        out[app] = {"learned_over_exhaustive_time": ratio, "timed": n,
+                    "distinct_plans": uniq,
+                    "replay_s": time.time() - t0}
+    return out
+
+
+def int_roofline(entry, int_peak):
+    """Integer-ALU roofline of the camera pipe: its kernel's integer
+    thread instructions per image (one ncu count of the default build,
+    profiles/counters.json) over the pipeline time, against the measured
+    integer throughput (polymage_b200.apps.measure.int_peak)."""
+    p = os.path.join(ROOT, "profiles", "counters.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f).get("campipe")
+    if not d:
+        return None
+    rate = d["integer_thread_inst"] / (entry["ms"] / 1e3)
+    peak = max(v["thread_inst_per_s"] for v in int_peak.values())
+    return {"integer_thread_inst_per_image": d["integer_thread_inst"],
+            "achieved_per_s": rate, "peak_per_s": peak,
+            "frac": rate / peak, "counted_on": d.get("kernel")}
+
+
 def run_reference_arm(args):
     ws, rank = _dist()
     if rank != 0:
@@ -383,6 +421,12 @@ def run(args):
                 measure.measure_bilateral_batch(64, device=dev)
             line["pipelines"]["stream1024"] = measure.measure_stream(
                 1024, device=dev)
+            ip = measure.int_peak(device=dev)
+            line["int_peak"] = ip
+            ir = int_roofline(line["pipelines"]["campipe"], ip)
+            if ir:
+                line["pipelines"]["campipe"]["int_roofline"] = ir
+            line["learned_vs_exhaustive"] = learned_vs_exhaustive()
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline()
             if "pipelines" in line:

@@ -672,6 +672,19 @@ class PipelineGen(object):
             w("const %s %s = %s.%s;" % (self.ptype(prm), self.pmap[prm], src,
                                         self.pmap[prm]))
 
+    def row_pitch(self, f):
+        """Elements the innermost rows of ``f`` are padded to a multiple
+        of in memory: 16 bytes' worth for an intermediate array of two or
+        more dimensions in the workspace (so that its rows are 16-byte
+        aligned and TMA can stage it), 1 for caller-owned inputs and
+        outputs and for const tables, which are dense."""
+        if any(f is x for x in self.inputs + self.outputs) or \
+                getattr(f, 'is_const_func', False) or \
+                len(f.domain) < 2 or f.typ.size() >= 16 or \
+                'no_row_pad' in self.p.options:
+            return 1
+        return 16 // f.typ.size()
+
     def declare_domain(self, w, f, ctx, need_strides):
         n = self.fn(f)
         dom = self.dom_exprs(f, ctx)
@@ -680,11 +693,17 @@ class PipelineGen(object):
                                                             hi))
         if need_strides:
             nd = len(dom)
+            pitch = self.row_pitch(f)
             w("const long long s_%s_%d = 1;" % (n, nd - 1))
             for d in range(nd - 2, -1, -1):
-                w("const long long s_%s_%d = s_%s_%d * (long long)"
-                  "(d_%s_hi%d - d_%s_lo%d + 1);" % (n, d, n, d + 1, n, d + 1,
-                                                    n, d + 1))
+                ext = "(long long)(d_%s_hi%d - d_%s_lo%d + 1)" % (
+                    n, d + 1, n, d + 1)
+                if d == nd - 2 and pitch > 1:
+                    # rows padded to 16 bytes (row_pitch)
+                    ext = "((%s + %d) / %d * %d)" % (ext, pitch - 1, pitch,
+                                                     pitch)
+                w("const long long s_%s_%d = s_%s_%d * %s;" % (
+                    n, d, n, d + 1, ext))
 
     def gindex(self, f, args, ctx, clamp_dd=True, clamp_all=False):
         """Linear index into a dense array of ``f`` at index ASTs ``args``;
@@ -827,9 +846,14 @@ class PipelineGen(object):
             w("{ size_t b = 0;")
             for comp in occ:
                 f = comp.func
-                ext = " * ".join("(size_t)pm_nonneg((%s) - (%s) + 1)" % (
+                exts = ["(size_t)pm_nonneg((%s) - (%s) + 1)" % (
                     ctx.expr(d.upperBound, {}), ctx.expr(d.lowerBound, {}))
-                    for d in f.domain)
+                    for d in f.domain]
+                pitch = self.row_pitch(f)
+                if pitch > 1:
+                    exts[-1] = "((%s + %d) / %d * %d)" % (
+                        exts[-1], pitch - 1, pitch, pitch)
+                ext = " * ".join(exts)
                 w("  { size_t e = (size_t)%d * %s; if (e > b) b = e; }" % (
                     f.typ.size(), ext))
             w("  off[%d] = o; o += pm_align256(b); }" % i)
@@ -2912,10 +2936,14 @@ class StencilGen(object):
             box = ", ".join(str(e) for e in n._sm_ext)
             w("{ long long dims[%d] = {%s}; int box[%d] = {%s};" % (
                 nd, dims, nd, box))
+            pitch = pg.row_pitch(f)
             w("  D.tma_%s = pm_use_tma() && pm_make_tmap(&D.tm_%s, D.b_%s, "
-              "%d, dims, box, %d, %d); }" % (
+              "%d, dims, box, %d, %d, %s); }" % (
                   nm, nm, pg.fn(f), nd, f.typ.size(),
-                  1 if f.typ in (C.Float, C.Double) else 0))
+                  1 if f.typ in (C.Float, C.Double) else 0,
+                  "(dims[%d] + %d) / %d * %d" % (nd - 1, pitch - 1, pitch,
+                                                 pitch) if pitch > 1
+                  else "dims[%d]" % (nd - 1)))
         w("return PM_OK;")
         w.close()
         w("")
@@ -3125,7 +3153,9 @@ class ReductionGen(object):
               "d_%s_lo%d; rr /= (d_%s_hi%d - d_%s_lo%d + 1);" % (
                   d, fnm, d, fnm, d, fnm, d, fnm, d, fnm, d))
         bind = dict(zip(f.variables, lv))
-        w("out[c] = (%s)(%s);" % (T, ctx0.expr(f.default, bind)))
+        w("out[%s] = (%s)(%s);" % (" + ".join(
+            "(long long)(q%d - d_%s_lo%d) * s_%s_%d" % (d, fnm, d, fnm, d)
+            for d in range(nd)), T, ctx0.expr(f.default, bind)))
         w.close()
         w.close()
         w.close()

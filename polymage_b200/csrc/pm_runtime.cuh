@@ -265,9 +265,11 @@ static CUtensorMapDataType pm_tma_dtype(int elem_size, int is_float) {
 // are given outermost first (C order); returns false when the TMA
 // preconditions do not hold (alignment, box limits), in which case the
 // kernel falls back to cooperative loads.
+// `pitch`: elements between the starts of consecutive innermost rows in
+// memory (dims[rank - 1] for a dense array; more for padded rows).
 static bool pm_make_tmap(CUtensorMap* m, const void* base, int rank,
                          const long long* dims, const int* box, int elem_size,
-                         int is_float) {
+                         int is_float, long long pitch) {
   memset(m, 0, sizeof(*m));
   pm_encode_tiled_fn fn = pm_get_encode_fn();
   if (!fn || rank < 1 || rank > 5) return false;
@@ -285,7 +287,8 @@ static bool pm_make_tmap(CUtensorMap* m, const void* base, int rank,
       if (stride % 16 != 0) return false;
       gstride[i - 1] = (cuuint64_t)stride;
     }
-    stride *= dims[c];
+    if (i == 0 && pitch < dims[c]) return false;
+    stride *= (i == 0) ? pitch : dims[c];
   }
   if ((bdim[0] * elem_size) % 16 != 0) return false;
   CUresult r = fn(m, pm_tma_dtype(elem_size, is_float), (cuuint32_t)rank,
