@@ -109,21 +109,33 @@ def nlmeans(pipe_data=None):
     out = Function(([c, x, y], [Interval(Int, 0, 2), rows, cols]), Float,
                    "non_local_means")
     out.defn = [Max(Min(nls(c, x, y) / nls(3, x, y), 1.0), 0.0)]
+    if pipe_data is not None:
+        pipe_data['pointwise'] = [dc, w, cwa]
     return out
 
 
 def build_nlmeans(rows=256, cols=256, patch_size=7, search_area=7,
                   tile_sizes=(16, 64), group_size=5,
-                  options=('oob_zero', ('red_tile', (8, 32, 1, 1, 16))),
-                  name="nlmeans"):
-    """Reductions are tiled (8, 32, 1, 1, 16) over their five reduction
-    variables: 8 x 32 pixels of one offset, and every channel, patch-window
-    tap or search offset along the last one."""
+                  options=('oob_zero',
+                           ('red_tile', (1, 16, 12, 12, 16)),
+                           ('red_tile:non_local_means_sum',
+                            (4, 2, 32, 12, 12))),
+                  inline=True, name="nlmeans"):
+    """The reductions are output-stationary: a thread owns cells of the
+    target and sums over the remaining reduction variable(s).  d, blur_d_y
+    and blur_d take tiles of 1 x 16 pixels x all 12 x 12 offsets (the
+    offsets innermost, as in memory); the weighted sum takes 4 channels x
+    2 x 32 pixels per tile and loops over the 144 offsets.  With
+    ``inline`` the pointwise stages dc, w and clamped_with_alpha are
+    substituted into their consumers (inline directives, as the
+    reference's compiler takes them) instead of being stored."""
     data = {}
     out = nlmeans(data)
     R, C = data['R'], data['C']
     ps, sa = data['patch_size'], data['search_area']
     return buildPipeline([out],
+                         inline_directives=data['pointwise'] if inline
+                         else [],
                          param_estimates=[(R, rows), (C, cols),
                                           (ps, patch_size),
                                           (sa, search_area)],

@@ -4,12 +4,13 @@
   python -m polymage_b200.autotune --app harris --learned model.npz --k 5
 
 Exhaustive mode runs ``tuner.generate`` + ``tuner.execute`` over the
-reference's search space (15 tile shapes x 5 group sizes, as the
-reference's app tuners use: harris/app_tuner.py:33-54) times the register
-blocking options, appending every measurement to the timing database.
+reference's search space (15 tile shapes x the 5 group sizes the
+reference's app tuners use, harris/app_tuner.py:33-54, plus 11, the size
+that fuses Harris whole) times the register blocking options, appending
+every measurement to the timing database.
 Learned mode ranks the same space with the cost model (pretrained on the
-other pipelines' measurements) and compiles and times only its top picks,
-in one round.
+other pipelines' measurements) and compiles and times only its top picks
+(8 by default), in one round.
 """
 
 import argparse
@@ -127,7 +128,7 @@ def main():
                     help='online learned tuning (cost model)')
     ap.add_argument('--compare', action='store_true',
                     help='learned tuning, then exhaustive tuning to compare')
-    ap.add_argument('--picks', type=int, default=14,
+    ap.add_argument('--picks', type=int, default=8,
                     help='configurations the learned tuner times (one '
                          'compile round)')
     ap.add_argument('--options', default=None,
@@ -151,6 +152,8 @@ def main():
                           shipped_app=args.app)
         out['learned'] = {'best': lr['best'], 'best_ms': lr['best_ms'],
                           'wall_s': lr['wall_s'], 'plan_s': lr['plan_s'],
+                          'compile_s': lr['compile_s'],
+                          'time_s': lr['time_s'],
                           'measured': len(lr['measured']),
                           'candidates': lr['candidates']}
     if not args.learned or args.compare:
@@ -158,6 +161,7 @@ def main():
                          option_configs=opts)
         best = rep['results'][0] if rep['results'] else None
         out['exhaustive'] = {'best': best, 'wall_s': rep['wall_s'],
+                             'generate_s': rep['generate_s'],
                              'n': len(rep['results'])}
     if args.compare and out['exhaustive']['best'] and \
             out['learned']['best_ms']:

@@ -610,6 +610,29 @@ def _cond_const_true(c, bind):
             '>': a > b, '>=': a >= b}.get(op, False)
 
 
+def _cond_static(c, bind):
+    """True / False when condition ``c`` has that value whatever the loop
+    variables are (after substituting ``bind``), else None."""
+    from .evaluate import try_eval_int
+    op = c.conditional
+    if op in ('&&', '||'):
+        a = _cond_static(c.lhs, bind)
+        b = _cond_static(c.rhs, bind)
+        if op == '&&':
+            if a is False or b is False:
+                return False
+            return True if (a and b) else None
+        if a is True or b is True:
+            return True
+        return False if (a is False and b is False) else None
+    a = try_eval_int(_subst(c.lhs, bind), {})
+    b = try_eval_int(_subst(c.rhs, bind), {})
+    if a is None or b is None:
+        return None
+    return {'==': a == b, '!=': a != b, '<': a < b, '<=': a <= b,
+            '>': a > b, '>=': a >= b}.get(op)
+
+
 def _const_int(e):
     """The value of an integer constant expression, else None."""
     try:
@@ -2354,9 +2377,24 @@ class StencilGen(object):
             return
         first = True
         for cond, expr, red in reversed(parts):
+            known = True if cond is None else _cond_static(cond, bind)
+            if known is False:
+                continue            # never holds at this point
+            if known is True and first:
+                # the last part that can hold always holds: no branch, and
+                # its reads stay in scope for the rest of the point (shared
+                # with the other channels of a channel block)
+                e = ctx.expr(expr, bind)
+                w("%s = (%s)(%s);" % (target, ctype(f.typ), e))
+                if written_flag:
+                    w("%s = true;" % written_flag)
+                return
             ctx.push()
-            c = ctx.cond(cond, bind) if cond is not None else "true"
-            w.open("%sif (%s)" % ("" if first else "else ", c))
+            if known is True:
+                w.open("else")
+            else:
+                c = ctx.cond(cond, bind)
+                w.open("%sif (%s)" % ("" if first else "else ", c))
             e = ctx.expr(expr, bind)
             w("%s = (%s)(%s);" % (target, ctype(f.typ), e))
             if written_flag:
@@ -2364,6 +2402,8 @@ class StencilGen(object):
             w.close()
             ctx.pop()
             first = False
+            if known is True:
+                return
 
     # ---- staging of external producers ------------------------------------------
     def gen_issue(self, bar):
@@ -2829,6 +2869,17 @@ class StencilGen(object):
                       "== 0%s;" % (fnm, "".join(
                           " && (s_%s_%d & 3) == 0" % (fnm, d)
                           for d in range(nd - 1))))
+        # channels tiled whole: on an interior tile the region spans the
+        # domain's constant channel range, so the channel of block member
+        # c is the literal lo + c and conditions on it fold at compile time
+        # (the camera pipe's per-channel colour matrix rows)
+        clo = None
+        if cb > 1 and self.inside:
+            from .tiling import _const_extent
+            lo0 = _const_int(f.domain[0].lowerBound)
+            if lo0 is not None and \
+                    _const_extent(f.domain[0], pg.p.int_env()) == cb:
+                clo = lo0
         group = []
         for c in range(cb):
             for k in range(K):
@@ -2838,8 +2889,11 @@ class StencilGen(object):
                     if nd >= 2 and k:
                         pt[nd - 2] = base[nd - 2] + k
                         qs[nd - 2] = "(qb%d + %d)" % (nd - 2, k)
-                    if c:
+                    if clo is not None:
+                        pt[0] = Value(clo + c, C.Int)
+                    elif c:
                         pt[0] = base[0] + c
+                    if c:
                         qs[0] = "(qb0 + %d)" % c
                     if u:
                         pt[nd - 1] = base[nd - 1] + u
@@ -3188,6 +3242,12 @@ class ReductionGen(object):
             w("const %s* __restrict__ b_%s = D.b_%s;" % (ctype(x.typ),
                                                          pg.fn(x), pg.fn(x)))
         w("%s* __restrict__ out = D.b_%s;" % (T, fnm))
+        if plan.gather is not None and not self.mixed:
+            self.gen_gather(ctx, parts)
+            w.close()
+            w("")
+            self.gen_launcher()
+            return
         priv = plan.privatize and not self.mixed
         if priv:
             # privatized box: union of target footprints of this tile
@@ -3297,6 +3357,94 @@ class ReductionGen(object):
         w.close()
         w("")
         self.gen_launcher()
+
+    def gen_gather(self, ctx, parts):
+        """Output-stationary accumulation (``plan.gather``): each thread
+        owns target cells of the tile -- the points of the reduction
+        variables that index the target -- and loops over the tile's range
+        of the other reduction variables, combining in a register.  When
+        the tile spans the whole range of those variables (one tile along
+        them, the usual case) the thread is the cell's only writer and
+        stores the default combined with its result; otherwise it combines
+        into the cell with one atomic."""
+        pg = self.pg
+        w = pg.w
+        plan = self.plan
+        f = self.f
+        fnm = pg.fn(f)
+        T = ctype(f.typ)
+        rvars = f.reductionVariables
+        nr = len(rvars)
+        tmap = plan.gather
+        outer = [d for d in range(nr) if tmap[d] is not None]
+        inner = [d for d in range(nr) if tmap[d] is None]
+        lv = _loop_vars(nr)
+        rbind = dict(zip(rvars, lv))
+        op = self.op
+
+        def combine(a, b):
+            # a and b are names or literals (evaluated once each)
+            if op == C.Op.Sum:
+                return "%s + %s" % (a, b)
+            if op == C.Op.Mul:
+                return "%s * %s" % (a, b)
+            # the atomics' rule: b replaces a when a < b (max), a > b (min)
+            return "(%s %s %s) ? %s : %s" % (
+                a, '<' if op == C.Op.Max else '>', b, b, a)
+
+        whole = " && ".join("D.gn[%d] == 1" % d for d in inner) or "true"
+        w("const bool pm_whole = %s;" % whole)
+        otile = [plan.tile[d] for d in outer]
+        tot = 1
+        for t in otile:
+            tot *= t
+        saved_lo = dict(ctx.var_lo)
+        for d, dom in enumerate(f.reductionDomain):
+            lo = _const_int(dom.lowerBound)
+            if lo is not None:
+                ctx.var_lo["q%d" % d] = lo
+        w.open("for (int i = threadIdx.x; i < %d; i += %d)" % (tot,
+                                                               plan.threads))
+        if outer:
+            StencilGen.decompose(self, "i", otile, "o")
+        for k, d in enumerate(outer):
+            w("const int q%d = a_lo%d + o%d;" % (d, d, k))
+        if outer:
+            w("if (%s) continue;" % " || ".join("q%d > a_hi%d" % (d, d)
+                                               for d in outer))
+        w("%s acc = %s;" % (T, self.identity()))
+        for d in inner:
+            w.open("for (int q%d = a_lo%d; q%d <= a_hi%d; ++q%d)" % (
+                d, d, d, d, d))
+        for cond, expr, red in parts:
+            tbind = tbind_of(f, rvars, red, rbind)
+            ctx.push()
+            w.open("")
+            cc = ctx.cond(cond, tbind) if cond is not None and \
+                not _cond_const_true(cond, tbind) else None
+            if cc is not None:
+                w.open("if (%s)" % cc)
+            w("const %s v = (%s)(%s);" % (T, T, ctx.expr(expr, rbind)))
+            w("acc = %s;" % combine("acc", "v"))
+            if cc is not None:
+                w.close()
+            w.close()
+            ctx.pop()
+        for d in inner:
+            w.close()
+        # the cell: target dimension t is indexed by reduction variable d
+        # with tmap[d] == t
+        cell = dict((tmap[d], "q%d" % d) for d in outer)
+        gidx = " + ".join("(long long)(%s - d_%s_lo%d) * s_%s_%d" % (
+            cell[t], fnm, t, fnm, t) for t in range(f.ndims))
+        dbind = dict((f.variables[tmap[d]], lv[d]) for d in outer)
+        w.open("if (pm_whole)")
+        w("const %s dflt = (%s)(%s);" % (T, T, ctx.expr(f.default, dbind)))
+        w("out[%s] = %s;" % (gidx, combine("dflt", "acc")))
+        w.close()
+        w("else %s(&out[%s], acc);" % (self.atomic(), gidx))
+        w.close()
+        ctx.var_lo = saved_lo
 
     def atomic(self, op=None):
         return {C.Op.Sum: 'pm_atomic_add', C.Op.Mul: 'pm_atomic_mul',

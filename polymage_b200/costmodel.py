@@ -338,7 +338,7 @@ class OnlineRanker(object):
             pred += m.predict(self.Xc)
         return [int(i) for i in np.argsort(pred)]
 
-    def run(self, cands, measure, batches=(14,), local=0):
+    def run(self, cands, measure, batches=(8,), local=0):
         for b in batches:
             pick = [i for i in self.order() if i not in self.measured][:b]
             if not pick:
@@ -356,7 +356,7 @@ class OnlineRanker(object):
         return min(ok, key=lambda i: self.measured[i]) if ok else None
 
 
-def learned_tune(arg_data, db_rows=None, batches=(14,), local=0,
+def learned_tune(arg_data, db_rows=None, batches=(8,), local=0,
                  ensemble=3, seed=0, shipped_app=None, measure=None):
     """Online learned tuning of one pipeline: plan every configuration of
     the search space (no compilation), keep one per distinct plan, then
@@ -391,13 +391,19 @@ def learned_tune(arg_data, db_rows=None, batches=(14,), local=0,
     Xb, yb = db_training_set(db_rows, exclude_app=app)
     t_plan = time.time() - t0
 
+    spent = {'compile_s': 0.0, 'time_s': 0.0}
+
     def default_measure(idx):
         b = dict(a)
         b['_tuner_configs'] = [cands[i] for i in idx]
+        t1 = time.time()
         src, n, pipe = tuner.generate(b)
+        t2 = time.time()
         b['_tuner_src_path'] = src
         b['_tuner_pipe'] = pipe
         rep = tuner.execute(b)
+        spent['compile_s'] += t2 - t1
+        spent['time_s'] += time.time() - t2
         got = dict((json.dumps([r['tile'], r['group_size'], r['options']]),
                     r['ms']) for r in rep['results'])
         return [got.get(json.dumps([cands[i]['tile'], cands[i]['group_size'],
@@ -413,10 +419,11 @@ def learned_tune(arg_data, db_rows=None, batches=(14,), local=0,
             'measured': [{'config': cands[i], 'ms': ms}
                          for i, ms in ranker.measured.items()],
             'candidates': len(cands), 'plan_s': t_plan,
+            'compile_s': spent['compile_s'], 'time_s': spent['time_s'],
             'wall_s': time.time() - t0}
 
 
-def evaluate_on_db(rows, app, batches=(14,), local=0, ensemble=3, seed=0):
+def evaluate_on_db(rows, app, batches=(8,), local=0, ensemble=3, seed=0):
     """Replay ``learned_tune`` on recorded measurements of ``app``: the
     ranker only learns the times of the configurations it picks.  Returns
     (best picked ms / best recorded ms, number measured, distinct plans)."""

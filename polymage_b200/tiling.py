@@ -272,10 +272,16 @@ class ReductionPlan(object):
         self.privatize = False
         self.smem_bytes = 0
         self.funcs = []
+        # output-stationary form: per reduction variable, the target
+        # dimension it indexes (None for the variables summed over), when
+        # every part targets the same cell given by plain reduction
+        # variables; None otherwise
+        self.gather = None
 
     def describe(self):
-        return ["reduction %s tile %s privatize %s ext %s" % (
-            self.func.name, self.tile, self.privatize, self.priv_ext)]
+        return ["reduction %s tile %s privatize %s ext %s gather %s" % (
+            self.func.name, self.tile, self.privatize, self.priv_ext,
+            self.gather)]
 
     def features(self):
         return {'nstages': 1, 'tile_inner': self.tile[-1],
@@ -354,12 +360,31 @@ def _refs_to(func, target):
 
 
 def plan_group(pipeline, group):
+    """Plan of one group of the final grouping.  A stencil group whose
+    tile needs more shared memory than the budget at the pipeline's tile
+    sizes (the 3-D multigrid's restriction and interpolation groups at
+    tiles that suit its smoothing steps) is planned with its largest tile
+    dimension halved until it fits.  Grouping decisions do not see this:
+    they are taken at the pipeline's tile sizes."""
     kind = group.kind
     if kind == 'const':
         return ConstPlan(group.comps[0].func)
     if kind == 'reduction':
         return plan_reduction(pipeline, group.comps)
-    return plan_stencil(pipeline, group.comps)
+    tile = None
+    while True:
+        try:
+            return plan_stencil(pipeline, group.comps, tile=tile)
+        except PlanError as e:
+            if 'exceeds budget' not in str(e) or \
+                    'no_tile_shrink' in pipeline.options:
+                raise
+            cur = list(tile or e.args[1])
+            big = max(range(len(cur)), key=lambda d: cur[d])
+            if cur[big] <= 1:
+                raise
+            cur[big] //= 2
+            tile = cur
 
 
 def check_group_plan(pipeline, comps):
@@ -370,7 +395,9 @@ def check_group_plan(pipeline, comps):
     plan_stencil(pipeline, comps)
 
 
-def plan_stencil(pipeline, comps):
+def plan_stencil(pipeline, comps, tile=None):
+    """Plan of a fused stencil group; ``tile`` overrides the tile the
+    pipeline's tile sizes give its anchor."""
     env = pipeline.int_env()
     pos = dict((c, i) for i, c in enumerate(pipeline.comps))
     comps = sorted(comps, key=lambda c: pos[c])
@@ -398,7 +425,8 @@ def plan_stencil(pipeline, comps):
     plan.threads = int(_option(pipeline, 'threads', DEFAULT_THREADS))
     budget = int(_option(pipeline, 'inline_budget', DEFAULT_INLINE_BUDGET))
     forced_smem = set(_option(pipeline, 'materialize', []) or [])
-    plan.tile = _tile_sizes_for(pipeline, anchor.ndims, anchor, env, funcs)
+    plan.tile = list(tile) if tile is not None else \
+        _tile_sizes_for(pipeline, anchor.ndims, anchor, env, funcs)
 
     # ---- materialization decisions, sinks first --------------------------
     uses = {}          # func -> [(M func, [arg exprs])]
@@ -556,7 +584,7 @@ def plan_stencil(pipeline, comps):
                  prefetch=('prefetch' in pipeline.options))
     if plan.smem_bytes > int(_option(pipeline, 'smem_budget', SMEM_BUDGET)):
         raise PlanError("shared memory %d B exceeds budget" %
-                        plan.smem_bytes)
+                        plan.smem_bytes, list(plan.tile))
     return plan
 
 
@@ -981,6 +1009,33 @@ def _layout_smem(plan, tight=False, env=None, prefetch=False):
 
 
 # ---------------------------------------------------------------------------
+def _gather_map(pipeline, f, rvars):
+    """Target dimension of each reduction variable when the reduction is
+    output-stationary: every part accumulates with the same operator into
+    the cell whose coordinates are plain reduction variables, the same
+    ones in every part and each at most once.  The other reduction
+    variables are then summed over inside one thread, with no atomics
+    (option 'no_gather' keeps the scatter form).  None otherwise."""
+    from .pipe import body_parts
+    if 'no_gather' in pipeline.options:
+        return None
+    parts = body_parts(f)
+    if len(set(red.op_type for _, _, red in parts)) != 1:
+        return None
+    tmap = None
+    for _, _, red in parts:
+        m = [None] * len(rvars)
+        for t, a in enumerate(red.accumulate_ref.arguments):
+            hit = [i for i, v in enumerate(rvars) if a is v]
+            if len(hit) != 1 or m[hit[0]] is not None:
+                return None
+            m[hit[0]] = t
+        if tmap is not None and m != tmap:
+            return None
+        tmap = m
+    return tmap
+
+
 def plan_reduction(pipeline, comps):
     from .pipe import body_parts
     if len(comps) != 1:
@@ -993,7 +1048,11 @@ def plan_reduction(pipeline, comps):
     plan.threads = int(_option(pipeline, 'threads', DEFAULT_THREADS))
     rvars = f.reductionVariables
     plan.tile = _tile_sizes_for(pipeline, len(rvars))
-    ts = _option(pipeline, 'red_tile')
+    # option ('red_tile:<name>', tile) for one reduction, else
+    # ('red_tile', tile) for all of them
+    ts = _option(pipeline, 'red_tile:' + f.name)
+    if ts is None:
+        ts = _option(pipeline, 'red_tile')
     if ts is not None:
         plan.tile = list(ts)[-len(rvars):]
     fns_all = []
@@ -1003,6 +1062,19 @@ def plan_reduction(pipeline, comps):
         fns_all.append([IndexFn(a, rvars)
                         for a in red.accumulate_ref.arguments])
     plan.target_fns = fns_all
+    plan.gather = _gather_map(pipeline, f, rvars)
+    if plan.gather is not None:
+        # each thread owns target cells and loops over the other reduction
+        # variables: their tile is their whole range at the parameter
+        # estimates (a call with a longer range splits it over tiles,
+        # which then combine with atomics)
+        for d, t in enumerate(plan.gather):
+            if t is None:
+                dom = f.reductionDomain[d]
+                ext = try_eval_int(dom.upperBound - dom.lowerBound + 1, env)
+                if ext is not None:
+                    plan.tile[d] = max(plan.tile[d], min(int(ext), 1 << 20))
+        return plan
     # privatized footprint of one tile, by simulation over a period
     divs = []
     for fns in fns_all:

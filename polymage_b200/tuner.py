@@ -33,7 +33,7 @@ from .tiling import PlanError
 DEFAULT_TILES = [[64, 256], [64, 128], [32, 512], [32, 256], [32, 128],
                  [32, 64], [16, 512], [16, 256], [16, 128], [16, 64],
                  [8, 512], [8, 256], [8, 128], [8, 64], [8, 32]]
-DEFAULT_GROUPS = [3, 5, 7, 9, 10]
+DEFAULT_GROUPS = [3, 5, 7, 9, 10, 11]
 
 
 def _log(dump, msg):

@@ -407,3 +407,27 @@ def test_tight_staging_of_interleaved_channels():
         else:
             assert '& ~15;' in seg
     assert loops[1] == 32 * 64 * 32 and loops[2] == 32 * 64 * 3
+
+
+def test_output_stationary_reductions():
+    """Reductions whose target cell is given by plain reduction variables
+    are planned output-stationary (each thread sums over the other
+    reduction variables, no atomics while one tile spans them); a
+    data-dependent target (the bilateral grid's intensity bin) keeps the
+    scatter form."""
+    from polymage_b200.apps.max_filter import build_maxfilter
+    from polymage_b200.apps.bilateral_grid import build_bilateral
+    plans = dict((g.plan.func.name, g.plan)
+                 for g in build_maxfilter().groups
+                 if g.plan.kind == 'reduction')
+    assert plans['final'].gather == [0, 1, 2, None]
+    assert plans['final'].tile[3] == 80          # dx spans [-26, 53]
+    assert plans['vert_log'].gather == [0, 1, 2, 3]
+    assert not plans['final'].privatize
+    bil = [g.plan for g in build_bilateral().groups
+           if g.plan.kind == 'reduction']
+    assert bil and all(p.gather is None for p in bil)
+    src = build_maxfilter().generate_code().source
+    k = src[src.index("pm_maxfilter_g4(const"):]
+    k = k[:k.index("\n}\n")]
+    assert "pm_whole" in k and "acc = (acc < v) ? v : acc;" in k

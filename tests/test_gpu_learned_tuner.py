@@ -3,8 +3,8 @@
 Replays the learned tuner on the committed B200 timing database (every
 configuration of the reference's search space, measured): for each pipeline
 the model is pretrained on the *other* pipelines only (on the GPU, by this
-package's kernels) and picks 14 configurations, which are then "timed" by
-looking them up.  Without the model, the same budget of 14 timed
+package's kernels) and picks 8 configurations, which are then "timed" by
+looking them up.  Without the model, the same budget of 8 timed
 configurations is spent on a random choice."""
 
 import numpy as np
@@ -21,9 +21,9 @@ def test_learned_beats_random_budget_and_reaches_near_best(cuda):
     assert len(apps) >= 5
     learned, random6 = [], []
     for app in apps:
-        ratio, n, uniq = costmodel.evaluate_on_db(rows, app, seed=0)
-
-        assert n == 14
+        ratio, n, uniq = costmodel.evaluate_on_db(rows, app, batches=(8,),
+                                                  seed=0)
+        assert n == 8
         learned.append(ratio)
         ms = {}
         for r in rows:
@@ -31,7 +31,7 @@ def test_learned_beats_random_budget_and_reaches_near_best(cuda):
                 k = costmodel.signature(r['features'], r)
                 ms[k] = min(ms.get(k, 1e9), r['ms'])
         v = np.array(list(ms.values()))
-        rnd = np.mean([np.random.default_rng(s).choice(v, 14, replace=False)
+        rnd = np.mean([np.random.default_rng(s).choice(v, 8, replace=False)
                        .min() / v.min() for s in range(300)])
         random6.append(rnd)
         print(app, "learned %.3f random %.3f (distinct plans %d)" % (
