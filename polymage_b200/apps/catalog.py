@@ -15,13 +15,22 @@ The bilateral grid's construction takes 16x256-pixel tiles (0.0908 vs
 0.1033 ms with 32x256), interpolation 32x64 tiles (0.53 vs 1.69 ms with
 the reference builder's 16x16).  The camera pipe fuses every stage into one
 group (option fuse_all; the greedy grouping leaves six kernels: 0.133 vs
-0.190 ms) on 64x128 tiles.  Harris,
-the camera pipe and both pyramids ask ptxas for 4 resident CTAs per SM
+0.190 ms) and tiles its three output channels whole (option channel_tile:
+a thread computes a pixel's red, green and blue once for all three
+channels, 0.085 vs 0.130 ms) on 32x128 tiles with 4 rows per thread.
+Harris and both pyramids ask ptxas for 4 resident CTAs per SM
 (``min_blocks=4``: at most 64 registers a thread), also outside the tuned
-space: 0.0290 vs 0.0303 ms, 0.185 vs 0.195 ms, 0.203 vs 0.209 ms and
+space: 0.0290 vs 0.0303 ms, 0.203 vs 0.209 ms and
 0.218 vs 0.227 ms (the 8-level pyramid with its interior tiles reading
 clamped taps unclamped); the bilateral grid is slower with it (0.108 vs
-0.107 ms) and unsharp is bound by shared memory, not registers."""
+0.107 ms) and unsharp is bound by shared memory, not registers.
+The widening pipelines' settings are the best of smaller sweeps
+(polymage_b200.apps.measure, same timing): Jacobi 2-D 32x64 tiles with 5
+steps per group (0.133 vs 0.207 ms for 16x64 with 10), Jacobi 3-D and the
+3-D multigrid cycles unfused (group size 1) on 8x16x32 and 8x16x64 tiles
+(0.164 vs 0.356 ms; 3.2 vs 8.6 ms): in 3-D the halo of a fused time step
+grows every face of a tile, so recomputation costs more than the HBM
+round trip it saves."""
 
 import functools
 
@@ -42,8 +51,8 @@ HARRIS = dict(tile_sizes=(32, 64), group_size=11,
               options=('rblock=8', 'min_blocks=4', 'threads=128'))
 UNSHARP = dict(tile_sizes=(64, 128), group_size=10,
                options=('rblock=16', 'inline_budget=400', 'threads=128'))
-CAMPIPE = dict(tile_sizes=(64, 128), group_size=12,
-               options=('rblock=8', 'min_blocks=4', 'fuse_all'))
+CAMPIPE = dict(tile_sizes=(32, 128), group_size=12,
+               options=('rblock=4', 'fuse_all', 'channel_tile'))
 BILATERAL = dict(tile_sizes=(1, 32, 128), group_size=10,
                  options=(('red_tile', (16, 256)), 'rblock=4'))
 PYRAMID = dict(tile_sizes=(32, 64), group_size=10,
@@ -62,13 +71,13 @@ LAPLACIAN = dict(tile_sizes=(32, 64), group_size=10, options=('rblock=8',))
 # (multigrid/jacobi{2D,3D}/Makefile:10-16), NAS MG class W (NAS-PB-MG-3.2/
 # Makefile:9), interpolation of a 2048x2048 RGBA image.
 INTERPOLATE = dict(rows=2048, cols=2048, tile_sizes=(32, 64), group_size=11)
-JACOBI2D = dict(N=2048, T=10, tile_sizes=(16, 64), group_size=10)
-JACOBI3D = dict(N=128, T=10, tile_sizes=(4, 8, 32), group_size=5)
+JACOBI2D = dict(N=2048, T=10, tile_sizes=(32, 64), group_size=5)
+JACOBI3D = dict(N=128, T=10, tile_sizes=(8, 16, 32), group_size=1)
 VCYCLE = dict(n=31, L=3, nu1=10, nu2=0, nuc=0, tile_sizes=(16, 64),
               group_size=6)
 WCYCLE = dict(VCYCLE, gamma=2, name="Wcycle")
 VCYCLE3D = dict(n=31, L=3, nu1=10, nu2=0, nuc=0, dims=3,
-                tile_sizes=(4, 8, 32), group_size=4, name="Vcycle3d")
+                tile_sizes=(8, 16, 64), group_size=1, name="Vcycle3d")
 WCYCLE3D = dict(VCYCLE3D, gamma=2, name="Wcycle3d")
 MG3P = dict(prob_class='W', tile_sizes=(4, 8, 32), group_size=6)
 # non-local means at the reference Makefile's patch size and search area
@@ -76,7 +85,9 @@ MG3P = dict(prob_class='W', tile_sizes=(4, 8, 32), group_size=6)
 NLMEANS = dict(rows=256, cols=256)
 # max filter (radius 26) on a 1536x2560 landscape image: the spec's
 # vert_log rows are [26, C-R-79], non-empty only when C > R + 104
-MAXFILTER = dict(rows=1536, cols=2560)
+# (tiles of 8 x 32 pixels x 3 channels for its reductions)
+MAXFILTER = dict(rows=1536, cols=2560,
+                 options=('oob_zero', ('red_tile', (8, 32, 3, 16))))
 
 _BUILDERS = {
     "harris": (build_harris, HARRIS),

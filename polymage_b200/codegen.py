@@ -3197,20 +3197,31 @@ class ReductionGen(object):
         pg.declare_params(w, "D")
         w("%s* __restrict__ out = D.b_%s;" % (T, fnm))
         pg.declare_domain(w, f, ctx0, True)
-        w.open("for (long long c = (long long)blockIdx.x * blockDim.x + "
-               "threadIdx.x; c < D.ncells; c += (long long)gridDim.x * "
-               "blockDim.x)")
-        w("long long rr = c;")
         lv = _loop_vars(nd)
-        for d in range(nd - 1, -1, -1):
-            w("const int q%d = (int)(rr %% (d_%s_hi%d - d_%s_lo%d + 1)) + "
-              "d_%s_lo%d; rr /= (d_%s_hi%d - d_%s_lo%d + 1);" % (
-                  d, fnm, d, fnm, d, fnm, d, fnm, d, fnm, d))
         bind = dict(zip(f.variables, lv))
-        w("out[%s] = (%s)(%s);" % (" + ".join(
-            "(long long)(q%d - d_%s_lo%d) * s_%s_%d" % (d, fnm, d, fnm, d)
-            for d in range(nd)), T, ctx0.expr(f.default, bind)))
-        w.close()
+        dflt = ctx0.expr(f.default, bind)
+        # cell index -> coordinates in 32-bit arithmetic when the domain
+        # has fewer than 2^31 cells (the usual case; 64-bit division is
+        # several times dearer), else in 64-bit
+        for IT in ("unsigned", "long long"):
+            if IT == "unsigned":
+                w.open("if (D.ncells <= 0x7fffffffLL)")
+            else:
+                w.open("else")
+            w.open("for (%s c = (%s)blockIdx.x * blockDim.x + threadIdx.x; "
+                   "c < (%s)D.ncells; c += (%s)gridDim.x * blockDim.x)" % (
+                       IT, IT, IT, IT))
+            w("%s rr = c;" % IT)
+            for d in range(nd - 1, -1, -1):
+                w("const int q%d = (int)(rr %% (%s)(d_%s_hi%d - d_%s_lo%d + "
+                  "1)) + d_%s_lo%d; rr /= (%s)(d_%s_hi%d - d_%s_lo%d + 1);"
+                  % (d, IT, fnm, d, fnm, d, fnm, d, IT, fnm, d, fnm, d))
+            w("out[%s] = (%s)(%s);" % (" + ".join(
+                "(long long)(q%d - d_%s_lo%d) * s_%s_%d" % (d, fnm, d, fnm,
+                                                             d)
+                for d in range(nd)), T, dflt))
+            w.close()
+            w.close()
         w.close()
         w.close()
         w("")
@@ -3517,6 +3528,21 @@ class ReductionGen(object):
                 i, i))
             w("D.gn[%d] = (D.ghi[%d] - D.glo[%d] + %d) / %d; tot *= D.gn[%d];"
               % (i, i, i, plan.tile[i], plan.tile[i], i))
+        if plan.gather is not None and not self.mixed:
+            # output-stationary: when the target variables' ranges cover
+            # the domain and one tile spans the summed ones, every cell is
+            # written once with its default folded in, and the init pass
+            # is skipped
+            cov = []
+            for d, t in enumerate(plan.gather):
+                if t is None:
+                    cov.append("D.gn[%d] == 1" % d)
+                else:
+                    dom = f.domain[t]
+                    cov.append("D.glo[%d] <= (%s) && D.ghi[%d] >= (%s)" % (
+                        d, ctx.expr(dom.lowerBound, {}), d,
+                        ctx.expr(dom.upperBound, {})))
+            w("if (%s) D.ncells = 0;" % " && ".join(cov))
         w("*ntiles = tot;")
         w("return PM_OK;")
         w.close()

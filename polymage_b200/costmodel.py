@@ -257,31 +257,40 @@ def plan_candidates(arg_data, configs, jobs=None, app_for_workers=None):
     the workers rebuild the spec by name); others sequentially."""
     import sys
     from . import tuner
+    name = arg_data.get('_tuner_pipe_name') or arg_data['_tuner_app_name']
+
+    def one(cfg):
+        try:
+            return tuner.pipeline_features(
+                tuner.plan_config(arg_data, cfg, name))
+        except Exception:
+            return None
+
+    if not configs:
+        return []
+    # the first plan, timed: a pool pays off only when planning them all
+    # one after another would take longer than starting its workers
+    t0 = time.time()
+    first = one(configs[0])
+    serial_s = (time.time() - t0) * len(configs)
     main_file = getattr(sys.modules.get('__main__'), '__file__', None)
     spawnable = main_file is not None and os.path.exists(main_file)
-    if app_for_workers is not None and len(configs) > 8 and spawnable:
+    if app_for_workers is not None and len(configs) > 8 and spawnable and \
+            serial_s > 4.0:
         import multiprocessing as mp
         jobs = jobs or max(1, (os.cpu_count() or 2) - 1)
         ctx = mp.get_context("spawn")
         pool = ctx.Pool(jobs)
         try:
             res = pool.map_async(_plan_worker,
-                                 [(app_for_workers, c) for c in configs],
+                                 [(app_for_workers, c) for c in configs[1:]],
                                  chunksize=max(1, len(configs) //
                                                (4 * jobs)))
-            return res.get(timeout=600)
+            return [first] + res.get(timeout=600)
         finally:
             pool.terminate()
             pool.join()
-    out = []
-    name = arg_data.get('_tuner_pipe_name') or arg_data['_tuner_app_name']
-    for cfg in configs:
-        try:
-            out.append(tuner.pipeline_features(
-                tuner.plan_config(arg_data, cfg, name)))
-        except Exception:
-            out.append(None)
-    return out
+    return [first] + [one(cfg) for cfg in configs[1:]]
 
 
 def _rblock(cfg):

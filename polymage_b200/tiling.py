@@ -508,9 +508,13 @@ def plan_stencil(pipeline, comps, tile=None):
         elif role[f] == 'smem':
             mk(f, 'smem')
     stage_inputs = 'no_stage' not in pipeline.options
+    # inputs read at one offset only are read straight from HBM, unless
+    # option 'stage_pointwise' asks for them to be staged by TMA too (the
+    # copy is then in flight while the tile's other stages compute)
+    min_mult = 1 if 'stage_pointwise' in pipeline.options else 2
     for x in externals:
         us = ext_uses[x]
-        want = stage_inputs and _multiplicity(us) >= 2 and \
+        want = stage_inputs and _multiplicity(us) >= min_mult and \
             not x.is_const_func
         if want:
             for m, args in us:
