@@ -12,7 +12,9 @@ tuned best); CTAs of 128 threads on 64x128 tiles with 16 rows per thread
 keep more, smaller CTAs resident (0.0773 vs 0.0866 ms with 256 threads).
 Harris also runs 128-thread CTAs, on 32x64 tiles (0.0273 vs 0.0291 ms).
 The bilateral grid's construction takes 16x256-pixel tiles (0.0908 vs
-0.1033 ms with 32x256), interpolation 32x64 tiles (0.53 vs 1.69 ms with
+0.1033 ms with 32x256), and its slicing group stages the input pixels by
+TMA although it reads each once (option stage_pointwise: 0.0728 vs 0.0786
+ms; the same option slows the pyramids and the local Laplacian), interpolation 32x64 tiles (0.53 vs 1.69 ms with
 the reference builder's 16x16).  The camera pipe fuses every stage into one
 group (option fuse_all; the greedy grouping leaves six kernels: 0.133 vs
 0.190 ms) and tiles its three output channels whole (option channel_tile:
@@ -54,7 +56,8 @@ UNSHARP = dict(tile_sizes=(64, 128), group_size=10,
 CAMPIPE = dict(tile_sizes=(32, 128), group_size=12,
                options=('rblock=4', 'fuse_all', 'channel_tile'))
 BILATERAL = dict(tile_sizes=(1, 32, 128), group_size=10,
-                 options=(('red_tile', (16, 256)), 'rblock=4'))
+                 options=(('red_tile', (16, 256)), 'rblock=4',
+                          'stage_pointwise'))
 PYRAMID = dict(tile_sizes=(32, 64), group_size=10,
                options=('rblock=8', 'min_blocks=4'))
 # 8 levels, indices clamped at every level's borders (any image size)

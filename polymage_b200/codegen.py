@@ -277,6 +277,14 @@ class ExprCtx(object):
             a = self.expr(e.true_expression, bind)
             b = self.expr(e.false_expression, bind)
             return "(%s ? %s : %s)" % (c, a, b)
+        if isinstance(e, (C.Pow, C.Powf)) and self.mode == 'device' and \
+                self._int_power_of_two(e):
+            # 2^n for an integer n is exact either way; ldexp scales by the
+            # exponent instead of evaluating a general power
+            n = self.expr(e.arguments[1], bind)
+            if isinstance(e, C.Powf):
+                return "ldexpf(1.0f, (int)(%s))" % n
+            return "ldexp(1.0, (int)(%s))" % n
         if isinstance(e, InbuiltFunction):
             args = []
             for a in e.arguments:
@@ -297,6 +305,19 @@ class ExprCtx(object):
                 args.append(t)
             return "%s(%s)" % (self._fname(e), ", ".join(args))
         raise CodegenError("cannot print %r" % (e,))
+
+    @staticmethod
+    def _int_power_of_two(e):
+        """Whether ``e`` is Pow(2, n) with n of a type whose every value
+        converts to int unchanged."""
+        b = Value.numericToValue(e.arguments[0])
+        if not (isinstance(b, Value) and b.value == 2):
+            return False
+        try:
+            t = getType(e.arguments[1])
+        except Exception:
+            return False
+        return t in (C.Int, C.Short, C.UShort, C.Char, C.UChar)
 
     def _fname(self, e):
         if isinstance(e, C.RandomFloat):
