@@ -65,7 +65,10 @@ PYRAMID8 = dict(L=8, tile_sizes=(32, 64), group_size=10,
                 options=('rblock=8', 'min_blocks=4'))
 
 # local Laplacian filter (the video demo's pipeline_laplacian), 1080p frames
-LAPLACIAN = dict(tile_sizes=(32, 64), group_size=10, options=('rblock=8',))
+# (option tight_stage: the uint8 [x][y][3] frame is staged without the TMA
+# alignment slack of its 3-byte innermost rows, 0.148 vs 0.213 ms)
+LAPLACIAN = dict(tile_sizes=(32, 64), group_size=10,
+                 options=('rblock=8', 'tight_stage'))
 
 # The widening pipelines at the reference Makefiles' settings: Jacobi 2-D
 # N=2048 and 3-D N=128 with 10 steps each (stencil/jacobi{2D,3D}/

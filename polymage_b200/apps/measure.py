@@ -170,7 +170,12 @@ def measure(app, steps=50, warmup=5, device=None, graph=True, warm=False,
     dev = device or torch.device("cuda", torch.cuda.current_device())
     cp = cp or catalog.build(app)
     prm, host_in, out_spec, pixels, desc = workload(app)
-    ins = dict((k, torch.from_numpy(v).to(dev)) for k, v in host_in.items())
+    # inputs that only const tables read (the camera pipe's two 3x4 colour
+    # matrices) stay in host memory, where the tables are computed
+    table_only = set(f.name for f in cp.inputs if id(f) in cp.table_only)
+    ins = dict((k, torch.from_numpy(v) if k in table_only
+                else torch.from_numpy(v).to(dev))
+               for k, v in host_in.items())
     outs = {}
     for k, (shape, dt) in out_spec.items():
         outs[k] = torch.zeros(shape, dtype=torch.from_numpy(

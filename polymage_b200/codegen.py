@@ -1406,7 +1406,8 @@ class PipelineGen(object):
     def gen_d2h(self, f, ctx, stream="s",
                 fail="{ pm_status = PM_ERR_CUDA; return; }", clip=None):
         """Copy the written points of output ``f`` back to the caller's
-        buffer (one 2-D copy per outer index); ``clip`` optionally
+        buffer (pm_copy_box_d2h: contiguous spans where the box covers
+        the inner dimensions whole, 2-D copies otherwise); ``clip`` optionally
         intersects the written box with per-dim (lo, hi) C expressions."""
         w = self.w
         n = self.fn(f)
@@ -1429,36 +1430,14 @@ class PipelineGen(object):
                 lo = "pm_llmax(%s, (long long)(%s))" % (lo, clip[d][0])
                 hi = "pm_llmin(%s, (long long)(%s))" % (hi, clip[d][1])
             w("const long long B%d_lo = %s, B%d_hi = %s;" % (d, lo, d, hi))
-        w("bool nonempty = %s;" % " && ".join(
-            "B%d_lo <= B%d_hi" % (d, d) for d in range(nd)))
-        w("long long S%d = 1;" % (nd - 1))
-        for d in range(nd - 2, -1, -1):
-            w("long long S%d = S%d * (D%d_hi - D%d_lo + 1);" % (d, d + 1,
-                                                                d + 1, d + 1))
-        w.open("if (nonempty)")
-        if nd == 1:
-            w("size_t o = (size_t)(B0_lo - D0_lo) * %d;" % es)
-            w("if (cudaMemcpyAsync((char*)%s + o, (char*)dv_%s + o, "
-              "(size_t)(B0_hi - B0_lo + 1) * %d, cudaMemcpyDeviceToHost, %s) "
-              "!= cudaSuccess) %s" % (f.name, n, es, stream, fail))
-        else:
-            # loops over the outer dims, one 2-D copy per outer point
-            for d in range(nd - 2):
-                w.open("for (long long i%d = B%d_lo; i%d <= B%d_hi; ++i%d)" % (
-                    d, d, d, d, d))
-            outer = " + ".join(["(i%d - D%d_lo) * S%d" % (d, d, d)
-                                for d in range(nd - 2)] or ["0"])
-            a, b = nd - 2, nd - 1
-            w("size_t o = (size_t)((%s) + (B%d_lo - D%d_lo) * S%d + (B%d_lo - "
-              "D%d_lo)) * %d;" % (outer, a, a, a, b, b, es))
-            w("size_t pitch = (size_t)S%d * %d;" % (a, es))
-            w("if (cudaMemcpy2DAsync((char*)%s + o, pitch, (char*)dv_%s + o, "
-              "pitch, (size_t)(B%d_hi - B%d_lo + 1) * %d, (size_t)(B%d_hi - "
-              "B%d_lo + 1), cudaMemcpyDeviceToHost, %s) != cudaSuccess) %s" % (
-                  f.name, n, b, b, es, a, a, stream, fail))
-            for d in range(nd - 2):
-                w.close()
-        w.close()
+        w("long long Dl[%d] = {%s}, Dh[%d] = {%s};" % (
+            nd, ", ".join("D%d_lo" % d for d in range(nd)), nd,
+            ", ".join("D%d_hi" % d for d in range(nd))))
+        w("long long Bl[%d] = {%s}, Bh[%d] = {%s};" % (
+            nd, ", ".join("B%d_lo" % d for d in range(nd)), nd,
+            ", ".join("B%d_hi" % d for d in range(nd))))
+        w("if (pm_copy_box_d2h(%s, dv_%s, %d, %d, Dl, Dh, Bl, Bh, %s)) %s" % (
+            f.name, n, es, nd, stream, fail))
         w.close()
 
     def gen_batch_entry(self):

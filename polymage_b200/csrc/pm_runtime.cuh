@@ -261,6 +261,55 @@ static CUtensorMapDataType pm_tma_dtype(int elem_size, int is_float) {
   }
 }
 
+// Device-to-host copy of the box [Bl, Bh] of a dense C-order array whose
+// domain is [Dl, Dh] (nd <= 8 dimensions, es-byte elements) into the same
+// positions of the host array.  The innermost dimensions the box covers
+// whole merge with the first one it does not into one contiguous span per
+// point of the dimensions outside it; the spans are the rows of 2-D copies
+// (one per point of the dimensions outside the rows' dimension), so an
+// interleaved [x][y][3] output written whole is one copy, not one 3-byte
+// row per pixel.  Returns 0, or 1 when a copy could not be issued.
+static int pm_copy_box_d2h(void* dst, const void* src, int es, int nd,
+                           const long long* Dl, const long long* Dh,
+                           const long long* Bl, const long long* Bh,
+                           cudaStream_t s) {
+  if (nd < 1 || nd > 8) return 1;
+  long long ext[8], S[8];
+  for (int d = 0; d < nd; ++d) {
+    if (Bl[d] > Bh[d]) return 0;
+    ext[d] = Dh[d] - Dl[d] + 1;
+  }
+  S[nd - 1] = 1;
+  for (int d = nd - 2; d >= 0; --d) S[d] = S[d + 1] * ext[d + 1];
+  int j = nd - 1;
+  while (j > 0 && Bl[j] == Dl[j] && Bh[j] == Dh[j]) --j;
+  const size_t span = (size_t)((Bh[j] - Bl[j] + 1) * S[j]) * es;
+  if (j == 0) {
+    const size_t o = (size_t)((Bl[0] - Dl[0]) * S[0]) * es;
+    return cudaMemcpyAsync((char*)dst + o, (const char*)src + o, span,
+                           cudaMemcpyDeviceToHost, s) != cudaSuccess;
+  }
+  // rows: dimension j - 1; one 2-D copy per point of the dimensions < j - 1
+  const int r = j - 1;
+  const size_t pitch = (size_t)S[r] * es;
+  const size_t rows = (size_t)(Bh[r] - Bl[r] + 1);
+  long long idx[8];
+  for (int d = 0; d < r; ++d) idx[d] = Bl[d];
+  while (true) {
+    long long off = (Bl[r] - Dl[r]) * S[r] + (Bl[j] - Dl[j]) * S[j];
+    for (int d = 0; d < r; ++d) off += (idx[d] - Dl[d]) * S[d];
+    const size_t o = (size_t)off * es;
+    if (cudaMemcpy2DAsync((char*)dst + o, pitch, (const char*)src + o, pitch,
+                          span, rows, cudaMemcpyDeviceToHost, s) !=
+        cudaSuccess)
+      return 1;
+    int d = r - 1;
+    while (d >= 0 && ++idx[d] > Bh[d]) { idx[d] = Bl[d]; --d; }
+    if (d < 0) break;
+  }
+  return 0;
+}
+
 // Encode a tiled tensor map over a dense row-major array.  `dims` and `box`
 // are given outermost first (C order); returns false when the TMA
 // preconditions do not hold (alignment, box limits), in which case the

@@ -38,6 +38,19 @@ class CompiledPipeline(object):
         self.name = module.name
         self.lib = ctypes.CDLL(so_path)
         self.params, self.inputs, self.outputs = pipeline.ordered_params()
+        # inputs read only by const tables (the camera pipe's colour
+        # matrices): the entry points tabulate them on the host, so they
+        # may stay in host memory also for the device entry points, where
+        # a device copy would cost a synchronous read-back every call
+        from .pipe import body_refs
+        readers = dict((id(f), []) for f in self.inputs)
+        for comp in pipeline.comps:
+            for r in body_refs(comp.func):
+                if id(r.objectRef) in readers:
+                    readers[id(r.objectRef)].append(comp)
+        self.table_only = set(
+            id(f) for f in self.inputs if readers[id(f)] and
+            all(c.is_const_func for c in readers[id(f)]))
         pt = [_ctype_of(p.typ) for p in self.params]
         vp = [ctypes.c_void_p] * (len(self.inputs) + len(self.outputs))
         n = self.name
@@ -154,7 +167,8 @@ class CompiledPipeline(object):
             t = (inputs if any(f is g for g in self.inputs) else outputs)[
                 f.name]
             shape = self.shape_of(f, params)
-            if not t.is_cuda or not t.is_contiguous():
+            if not t.is_contiguous() or not t.is_cuda and \
+                    id(f) not in self.table_only:
                 raise TypeError("%s must be a contiguous CUDA tensor" % f.name)
             if t.numel() != int(np.prod(shape)):
                 raise ValueError("%s must have %d elements" % (

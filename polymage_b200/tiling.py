@@ -316,8 +316,10 @@ def _tile_sizes_for(pipeline, ndims, anchor=None, env=None, funcs=()):
     tiled whole when the group computes stages of fewer dimensions than the
     anchor (the camera pipe's red, green and blue planes feeding every
     output channel): one tile then computes them once for all channels
-    instead of once per channel (option 'channel_tile'; measured slower
-    on the camera pipe, 0.207 vs 0.190 ms, and the pyramids)."""
+    instead of once per channel (option 'channel_tile'); option
+    'channel_tile_all' tiles such a channel dimension whole in every group,
+    so that the channels of a point share their index arithmetic and the
+    lower-dimensional inputs they read."""
     ts = list(pipeline.tile_sizes)
     opt = _option(pipeline, 'tile')
     if opt is not None:
@@ -333,8 +335,9 @@ def _tile_sizes_for(pipeline, ndims, anchor=None, env=None, funcs=()):
     head = [int(t) for t in ts[max(0, len(ts) - n):]]
     lead = [1] * (n - len(head))
     if lead and not tail and env is not None and \
-            'channel_tile' in pipeline.options and \
-            any(f.ndims < ndims for f in funcs if f is not anchor):
+            ('channel_tile' in pipeline.options and
+             any(f.ndims < ndims for f in funcs if f is not anchor) or
+             'channel_tile_all' in pipeline.options):
         e = _const_extent(anchor.domain[0], env)
         if e is not None and e <= 4:
             lead[0] = int(e)

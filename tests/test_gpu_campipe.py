@@ -49,6 +49,31 @@ def test_campipe_device_abi_params_change(cp, cuda):
         assert np.array_equal(out.cpu().numpy(), ref)
 
 
+def test_campipe_device_abi_host_matrices(cp, cuda):
+    """The colour matrices feed only a const table, so the device entry
+    takes them in host memory (no read-back per call); a matrix edited in
+    place between calls is seen by the next call."""
+    import torch
+    R, C = 260, 388
+    img = OC.make_input(R, C, seed=11)
+    t_img = torch.from_numpy(img).to(cuda)
+    m3 = torch.from_numpy(OC.MATRIX_3200.copy())
+    m7 = torch.from_numpy(OC.MATRIX_7000.copy())
+    prm = {'C': C, 'R': R, 'colour_temp': 4500.0, 'contrast': 50.0,
+           'gamma': 2.0}
+    for step in range(2):
+        if step:
+            m3[0, 0] += 0.25
+        out = torch.zeros((3, R - 48, C - 64), dtype=torch.uint8,
+                          device=cuda)
+        cp.run_dev(prm, {'img': t_img, 'matrix_3200': m3,
+                         'matrix_7000': m7}, {'process': out})
+        torch.cuda.synchronize()
+        cp.check()
+        ref = OC.campipe(img, 4500.0, 50.0, 2.0, m3200=m3.numpy())
+        assert np.array_equal(out.cpu().numpy(), ref)
+
+
 def test_campipe_too_small_refused(cp):
     from polymage_b200.runtime import PipelineRuntimeError
     R, C = 40, 50          # no output domain; the raw is smaller than the
