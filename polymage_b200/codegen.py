@@ -3179,6 +3179,7 @@ class ReductionGen(object):
         w("int glo[%d], ghi[%d], gn[%d];" % (nr, nr, nr))
         w("int tile_base;")
         w("long long ncells;")
+        w("long long nbytes;     // the array's bytes, row padding included")
         w.close("};")
         w.open("struct %s_launch" % k)
         w("%s_desc d0;" % k)
@@ -3297,7 +3298,20 @@ class ReductionGen(object):
             w("#pragma unroll %d" % un)
         w.open("for (int i = threadIdx.x; i < %d; i += %d)" % (tot,
                                                                plan.threads))
-        StencilGen.decompose(self, "i", plan.tile, "j")
+        spread = self.spread_factor()
+        if spread:
+            # option 'red_spread': consecutive threads take points k apart
+            # along the innermost reduction variable (k = the divisor that
+            # maps it to a target cell), so that a warp's 32 atomics go to
+            # 32 different cells instead of 32/k threads per cell
+            E = plan.tile[-1]
+            m = E // spread
+            w("const int pm_ii = i %% %d;" % E)
+            w("const int pm_is = (i - pm_ii) + (pm_ii %% %d) * %d + "
+              "pm_ii / %d;" % (m, spread, m))
+            StencilGen.decompose(self, "pm_is", plan.tile, "j")
+        else:
+            StencilGen.decompose(self, "i", plan.tile, "j")
         lv = _loop_vars(nr)
         for d in range(nr):
             w("const int q%d = a_lo%d + j%d;" % (d, d, d))
@@ -3368,6 +3382,32 @@ class ReductionGen(object):
         w.close()
         w("")
         self.gen_launcher()
+
+    def zero_default(self):
+        """Whether the reduction's default is the constant 0 (all-zero
+        bytes for every element type used here)."""
+        d = Value.numericToValue(self.f.default)
+        return isinstance(d, Value) and d.value == 0
+
+    def spread_factor(self):
+        """With option 'red_spread': the divisor k by which the innermost
+        reduction variable indexes the target (a grid cell of k points),
+        when the tile along it holds at least 32 cells of k; else 0."""
+        if 'red_spread' not in self.pg.p.options:
+            return 0
+        from .evaluate import divisors_in
+        plan = self.plan
+        rv = self.f.reductionVariables[-1]
+        ks = set()
+        for fns in plan.target_fns:
+            for fn in fns:
+                if fn.kind == 'mono' and fn.var is rv:
+                    ks.update(divisors_in(fn.expr))
+        if len(ks) != 1:
+            return 0
+        k = ks.pop()
+        E = plan.tile[-1]
+        return k if k > 1 and E % k == 0 and E // k >= 32 else 0
 
     def gen_gather(self, ctx, parts):
         """Output-stationary accumulation (``plan.gather``): each thread
@@ -3519,6 +3559,14 @@ class ReductionGen(object):
         for d in f.domain:
             w("D.ncells *= (long long)pm_nonneg((%s) - (%s) + 1);" % (
                 ctx.expr(d.upperBound, {}), ctx.expr(d.lowerBound, {})))
+        pitch = pg.row_pitch(f)
+        exts = ["(long long)pm_nonneg((%s) - (%s) + 1)" % (
+            ctx.expr(d.upperBound, {}), ctx.expr(d.lowerBound, {}))
+            for d in f.domain]
+        if pitch > 1:
+            exts[-1] = "((%s + %d) / %d * %d)" % (exts[-1], pitch - 1, pitch,
+                                                  pitch)
+        w("D.nbytes = (long long)%d * %s;" % (f.typ.size(), " * ".join(exts)))
         w("long long tot = 1;")
         for i, d in enumerate(f.reductionDomain):
             lo = ctx.expr(d.lowerBound, {})
@@ -3554,8 +3602,14 @@ class ReductionGen(object):
         w("L.nimg = 1;")
         w("long long nt = 0;")
         w("int st = %s(L.d0, A, wsoff, &nt); if (st) return st;" % fill)
-        w("if (L.d0.ncells > 0) %s_init<<<(unsigned)pm_llmin((L.d0.ncells + "
-          "255) / 256, 148LL * 16), 256, 0, s>>>(L);" % k)
+        if self.zero_default():
+            # a default of 0: the init pass is a memset of the array (its
+            # row padding included)
+            w("if (L.d0.ncells > 0 && cudaMemsetAsync(L.d0.b_%s, 0, (size_t)"
+              "L.d0.nbytes, s) != cudaSuccess) return PM_ERR_CUDA;" % fnm)
+        else:
+            w("if (L.d0.ncells > 0) %s_init<<<(unsigned)pm_llmin((L.d0.ncells"
+              " + 255) / 256, 148LL * 16), 256, 0, s>>>(L);" % k)
         w("if (nt == 0) return cudaGetLastError() == cudaSuccess ? PM_OK : "
           "PM_ERR_CUDA;")
         w.open("if (!%s_attr[pm_cur_dev()])" % k)
