@@ -32,7 +32,11 @@ steps per group (0.133 vs 0.207 ms for 16x64 with 10), Jacobi 3-D and the
 3-D multigrid cycles unfused (group size 1) on 8x16x32 and 8x16x64 tiles
 (0.164 vs 0.356 ms; 3.2 vs 8.6 ms): in 3-D the halo of a fused time step
 grows every face of a tile, so recomputation costs more than the HBM
-round trip it saves."""
+round trip it saves.  The Jacobi steps, the 2-D multigrid cycles and NAS MG
+also stage their pointwise-read right-hand sides by TMA (option
+stage_pointwise: Jacobi 2-D 0.116 vs 0.132 ms, 3-D 0.154 vs 0.165 ms,
+V-cycle 0.073 vs 0.083 ms, W-cycle 0.138 vs 0.155 ms, NAS MG 0.255 vs
+0.264 ms; the 3-D cycles are slower with it)."""
 
 import functools
 
@@ -77,15 +81,18 @@ LAPLACIAN = dict(tile_sizes=(32, 64), group_size=10,
 # (multigrid/jacobi{2D,3D}/Makefile:10-16), NAS MG class W (NAS-PB-MG-3.2/
 # Makefile:9), interpolation of a 2048x2048 RGBA image.
 INTERPOLATE = dict(rows=2048, cols=2048, tile_sizes=(32, 64), group_size=11)
-JACOBI2D = dict(N=2048, T=10, tile_sizes=(32, 64), group_size=5)
-JACOBI3D = dict(N=128, T=10, tile_sizes=(8, 16, 32), group_size=1)
+JACOBI2D = dict(N=2048, T=10, tile_sizes=(32, 64), group_size=5,
+                options=('stage_pointwise',))
+JACOBI3D = dict(N=128, T=10, tile_sizes=(8, 16, 32), group_size=1,
+                options=('stage_pointwise',))
 VCYCLE = dict(n=31, L=3, nu1=10, nu2=0, nuc=0, tile_sizes=(16, 64),
-              group_size=6)
+              group_size=6, options=('stage_pointwise',))
 WCYCLE = dict(VCYCLE, gamma=2, name="Wcycle")
 VCYCLE3D = dict(n=31, L=3, nu1=10, nu2=0, nuc=0, dims=3,
                 tile_sizes=(8, 16, 64), group_size=1, name="Vcycle3d")
 WCYCLE3D = dict(VCYCLE3D, gamma=2, name="Wcycle3d")
-MG3P = dict(prob_class='W', tile_sizes=(4, 8, 32), group_size=6)
+MG3P = dict(prob_class='W', tile_sizes=(4, 8, 32), group_size=6,
+            options=('stage_pointwise',))
 # non-local means at the reference Makefile's patch size and search area
 # (non_local_means/Makefile:11-12) on a 256x256 image
 NLMEANS = dict(rows=256, cols=256)
