@@ -118,6 +118,38 @@ def auto_group(pipeline):
             break
 
 
+def merge_small(pipeline, limit):
+    """Option ('merge_small', N): after the greedy grouping, a group whose
+    only child group is C merges into C when every stage of both has at
+    most N points (at the parameter estimates) and the merged group has a
+    legal plan, whatever the group size.  A single child keeps the merged
+    group convex.  Meant for the coarse levels of pyramids, where each
+    level's kernel is short and the chain of launches is the cost."""
+    _, sizes = get_small_comps(pipeline)
+
+    def small(g):
+        return all(sizes.get(c) is not None and sizes[c] <= limit
+                   for c in g.comps)
+
+    changed = True
+    while changed:
+        changed = False
+        for group in list(pipeline.groups):
+            if len(group.children) != 1:
+                continue
+            ch = group.children[0]
+            if any(c.is_reduction or c.is_const_func
+                   for c in group.comps + ch.comps):
+                continue
+            if not (small(group) and small(ch)):
+                continue
+            if not _plan_ok(pipeline, list(group.comps) + list(ch.comps)):
+                continue
+            pipeline.merge_groups(group, ch)
+            changed = True
+            break
+
+
 def fuse_all(pipeline):
     """Option 'fuse_all': after the greedy grouping, put every stage that is
     neither a Reduction nor a const function into one group, when that

@@ -323,6 +323,9 @@ class Pipeline(object):
             grouping.manual_group(self, self._grouping)
         else:
             grouping.auto_group(self)
+            ms = tiling._option(self, 'merge_small')
+            if ms:
+                grouping.merge_small(self, int(ms))
             if 'fuse_all' in self._options:
                 grouping.fuse_all(self)
         schedule.schedule_groups(self)
