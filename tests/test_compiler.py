@@ -431,3 +431,54 @@ def test_output_stationary_reductions():
     k = src[src.index("pm_maxfilter_g4(const"):]
     k = k[:k.index("\n}\n")]
     assert "pm_whole" in k and "acc = (acc < v) ? v : acc;" in k
+
+
+def test_tile_shrinks_for_groups_over_the_shared_memory_budget():
+    """The 3-D V-cycle at 8x16x64 tiles: its smoothing groups plan at the
+    pipeline's tile sizes, while the restriction / interpolation groups
+    that would need more shared memory than the budget are planned with
+    halved tiles; option 'no_tile_shrink' refuses the plan instead."""
+    from polymage_b200.apps.multigrid import build_v_cycle
+    kw = dict(n=15, L=2, nu1=2, nu2=0, nuc=0, dims=3,
+              tile_sizes=(8, 16, 64), group_size=1, name="Vcycle3d_t")
+    p = build_v_cycle(**kw)
+    tiles = [tuple(g.plan.tile) for g in p.groups
+             if g.plan.kind == 'stencil']
+    assert (8, 16, 64) in tiles
+    assert any(t != (8, 16, 64) for t in tiles)
+    for g in p.groups:
+        if g.plan.kind == 'stencil':
+            assert g.plan.smem_bytes <= 200 * 1024
+    with pytest.raises(PlanError):
+        build_v_cycle(**dict(kw, options=('no_tile_shrink',)))
+
+
+def test_zero_default_reductions_start_from_a_memset():
+    """A Reduction whose default is 0 (the bilateral grid) is cleared with
+    cudaMemsetAsync in the single-image entry; the batched path keeps its
+    init kernel."""
+    from polymage_b200.apps.bilateral_grid import build_bilateral
+    src = build_bilateral().generate_code().source
+    launcher = src[src.index("static int launch_pm_bilateral_g0("):]
+    launcher = launcher[:launcher.index("\n}\n")]
+    assert "cudaMemsetAsync(L.d0.b_grid, 0, (size_t)L.d0.nbytes, s)" in \
+        launcher
+    assert "_init<<<" not in launcher
+    assert "pm_bilateral_g0_init<<<" in src          # batches
+
+
+def test_whole_channel_tiles_fold_channel_conditions():
+    """With option channel_tile the camera pipe's output group computes
+    the three channels of a pixel in one thread; on interior tiles the
+    channel index is a literal, so the colour correction's
+    Case(c == k) parts leave no runtime channel test behind and the
+    channels share the demosaicked values."""
+    from polymage_b200.apps import catalog
+    b, kw = catalog._BUILDERS['campipe']
+    assert 'channel_tile' in kw['options']
+    src = b(**kw).generate_code().source
+    k = src[src.index("// stage process"):]
+    fast = k[k.index("if (pm_inside)"):]
+    fast = fast[:fast.index("\n      }\n      else")]
+    assert "== 2)" not in fast and "== 1)" not in fast
+    assert fast.count("b_process[gb") == fast.count("b_process[")
