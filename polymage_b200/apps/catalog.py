@@ -136,3 +136,13 @@ def build(name):
         b, kw = _BUILDERS[name]
         _cache[name] = b(**kw).build()
     return _cache[name]
+
+
+def variant(name, extra_options=(), drop_options=()):
+    """The uncompiled pipeline of a shipped build with options added
+    (``extra_options``) or removed (``drop_options``)."""
+    b, kw = _BUILDERS[name]
+    kw = dict(kw)
+    opts = [o for o in kw.get('options', ()) if o not in drop_options]
+    kw['options'] = tuple(opts) + tuple(extra_options)
+    return b(**kw)

@@ -213,8 +213,7 @@ def measure(app, steps=50, warmup=5, device=None, graph=True, warm=False,
             "ms_min": per[0], "ms_median": float(np.median(per)),
             "ms_max": per[-1],
             "mpix_s": pixels / (ms / 1e3) / 1e6,
-            "launches": sum({'stencil': 1, 'reduction': 2}.get(g['kind'], 0)
-                            for g in cp.module.meta.get('groups', [])),
+            "launches": cp.module.meta.get('launches'),
             "entry": "pipeline_%s_%s" % (cp.name, "graph" if graph else "dev"),
             "compulsory_bytes": int(nbytes), "achieved_gbs": gbs,
             "hbm_frac": gbs / peak, "peak_gbs": peak, "peak_source": kind,
@@ -382,6 +381,9 @@ def main():
                     help="end to end through the host-buffer C ABI")
     ap.add_argument("--int-peak", action="store_true",
                     help="integer-ALU throughput of the GPU")
+    ap.add_argument("--options", default=None,
+                    help="JSON list of options added to the catalog build "
+                         "(e.g. '[\"chain\"]')")
     args = ap.parse_args()
     if args.int_peak:
         print(json.dumps(int_peak()))
@@ -395,8 +397,15 @@ def main():
         elif args.host:
             print(json.dumps(measure_host(app, min(args.steps, 20))))
         else:
-            print(json.dumps(measure(app, args.steps, args.warmup,
-                                     warm=args.warm)))
+            cp = None
+            if args.options:
+                opts = [tuple(o) if isinstance(o, list) else o
+                        for o in json.loads(args.options)]
+                cp = catalog.variant(app, opts).build()
+            r = measure(app, args.steps, args.warmup, warm=args.warm, cp=cp)
+            if args.options:
+                r["options"] = json.loads(args.options)
+            print(json.dumps(r))
 
 
 if __name__ == "__main__":

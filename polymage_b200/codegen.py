@@ -950,24 +950,28 @@ class PipelineGen(object):
                     reads.add(k)
         return reads, writes
 
-    def schedule(self):
+    def schedule(self, batch=False):
         """(stream of each launch, waits, recorded launches) of the
-        concurrent schedule (polymage_b200.streams)."""
-        if getattr(self, '_sched', None) is None:
+        concurrent schedule (polymage_b200.streams).  ``batch``: the
+        batched entries' launches, one per group (no chains)."""
+        key = '_bsched' if batch else '_sched'
+        if getattr(self, key, None) is None:
             from . import streams
             nst = int(_opt(self.p, 'streams', DEFAULT_STREAMS))
-            self._sched = streams.schedule(self.launch_rw, nst,
-                                           main_only=self.launch_main)
-        return self._sched
+            rw, main = (self.group_launch_rw, self.group_launch_main) \
+                if batch else (self.launch_rw, self.launch_main)
+            setattr(self, key, streams.schedule(rw, nst, main_only=main))
+        return getattr(self, key)
 
-    def emit_calls(self, w, calls, ret):
+    def emit_calls(self, w, calls, ret, batch=False):
         """Every group's launch in program order, spread over concurrent
         streams when groups are independent.  ``calls[j]``: the C call of
         launch j with ``{s}`` where its stream goes (it returns a status);
         ``ret``: the statement that returns a failed ``st``.  The caller's
         stream ``s`` forks to the side streams first and joins them at the
-        end, also when a launch fails."""
-        sof, waits, records = self.schedule()
+        end, also when a launch fails.  ``batch``: the calls are the
+        batched entries' per-group launches."""
+        sof, waits, records = self.schedule(batch)
         used = sorted(set(sof) - {0})
         if not used:
             for c in calls:
@@ -1488,7 +1492,7 @@ class PipelineGen(object):
         w("int st = 0;")
         self.emit_calls(w, ["%s(nullptr, nullptr, 0, n, nullptr, nullptr, "
                             "nullptr, {s}, 1)" % f for f in self.batch_fns],
-                        "return pm_status = st;")
+                        "return pm_status = st;", batch=True)
         w("return pm_status = PM_OK;")
         w.close()
         w("pm_batch_key.clear(); pm_batch_ws = nullptr;")
@@ -1538,7 +1542,7 @@ class PipelineGen(object):
                             "pm_batch_pinned, ddesc, &doff, {s}, 0)" % (
                                 f, max(self.nslots, 1))
                             for f in self.batch_fns],
-                        "return pm_status = st;")
+                        "return pm_status = st;", batch=True)
         w("// the pinned descriptors are free once every stream's upload is")
         w("cudaEventRecord(pm_batch_event[dev], s);")
         w("pm_batch_key = key; pm_batch_ws = ws;")
@@ -1816,16 +1820,34 @@ class StencilGen(object):
         plan = self.plan
         w = pg.w
         k = self.k
-        anchor = plan.anchor
-        na = anchor.ndims
         nt = plan.threads
         # option 'min_blocks=N': ask ptxas for N resident CTAs per SM
         # (caps registers per thread)
         mb = int(_opt(pg.p, 'min_blocks', 0) or 0)
         lb = "%d, %d" % (nt, mb) if mb > 0 else "%d" % nt
+        self.launch_bounds = lb
+        # The group's work is a device function over the launch's tiles
+        # [first, total): CTA ``pm_bid`` of ``pm_nb`` takes tile first +
+        # pm_bid, then every pm_nb-th (stride) or the queue's next.  The
+        # group's own kernel calls it with PM_CH false; a chain kernel
+        # (several groups in one launch) with PM_CH true.
+        w("template <bool PM_CH>")
+        w("static __device__ __forceinline__ void %s_body(const %s_launch& L,"
+          " const int pm_bid, const int pm_nb)" % (k, k))
+        w.open("")
+        self.gen_body()
+        w.close()
         w('extern "C" __global__ void __launch_bounds__(%s) %s(const '
           '__grid_constant__ %s_launch L)' % (lb, k, k))
         w.open("")
+        w("%s_body<false>(L, (int)blockIdx.x, (int)gridDim.x);" % k)
+        w.close()
+        w("")
+
+    def gen_body(self):
+        pg = self.pg
+        plan = self.plan
+        w = pg.w
         w("extern __shared__ __align__(128) unsigned char pm_smem[];")
         # option 'prefetch': the next tile's staged inputs are loaded into
         # a second copy of their buffers while this tile computes
@@ -1853,12 +1875,11 @@ class StencilGen(object):
             w("uint32_t pm_phase = 0;")
         w("__shared__ int pm_next_tile;")
         if not pre:
-            w("// Tiles: blockIdx.x first; with a tile queue (persistent "
+            w("// Tiles: pm_bid first; with a tile queue (persistent "
               "launch)")
             w("// each CTA then takes the next index from the device "
               "counter.")
-            w.open("for (int tile = L.first + (int)blockIdx.x; tile < "
-                   "L.total; )")
+            w.open("for (int tile = L.first + pm_bid; tile < L.total; )")
             self.gen_tile_setup("tile")
             self.gen_buffers(None)
             if self.stage_nodes:
@@ -1874,15 +1895,14 @@ class StencilGen(object):
             w("__syncthreads();      // shared memory is reused by the next "
               "tile")
             w.open("if (L.queue)")
-            w("if (threadIdx.x == 0) pm_next_tile = L.first + (int)gridDim.x"
-              " + atomicAdd(L.queue, 1);")
+            w("if (threadIdx.x == 0) pm_next_tile = L.first + pm_nb + "
+              "atomicAdd(L.queue, 1);")
             w("__syncthreads();")
             w("tile = pm_next_tile;")
             w.close()
-            w("else tile += (int)gridDim.x;")
+            w("else tile += pm_nb;")
             w.close()
-            w.close()
-            w("")
+            self.gen_body_end()
             return
         # Prefetching tile loop: the staged inputs of a CTA's tiles
         # alternate between two copies; the loads of tile n+1 are issued
@@ -1890,7 +1910,7 @@ class StencilGen(object):
         # from the queue one tile ahead.
         w("int pm_buf = 0;          // copy of the staged inputs this tile "
           "reads")
-        w("int tile = L.first + (int)blockIdx.x;")
+        w("int tile = L.first + pm_bid;")
         w("bool pm_pend = false;    // loads in flight into the other copy")
         w.open("if (tile < L.total)")
         self.gen_tile_setup("tile")
@@ -1900,12 +1920,12 @@ class StencilGen(object):
         w.open("while (tile < L.total)")
         w("int pm_nt = L.total;")
         w.open("if (L.queue)")
-        w("if (threadIdx.x == 0) pm_next_tile = L.first + (int)gridDim.x + "
+        w("if (threadIdx.x == 0) pm_next_tile = L.first + pm_nb + "
           "atomicAdd(L.queue, 1);")
         w("__syncthreads();")
         w("pm_nt = pm_next_tile;")
         w.close()
-        w("else if (L.stride) pm_nt = tile + (int)gridDim.x;")
+        w("else if (L.stride) pm_nt = tile + pm_nb;")
         w("pm_pend = false;")
         w.open("if (pm_nt < L.total)")
         self.gen_tile_setup("pm_nt")
@@ -1926,8 +1946,22 @@ class StencilGen(object):
         w("pm_buf ^= 1;")
         w("tile = pm_nt;")
         w.close()
+        self.gen_body_end()
+
+    def gen_body_end(self):
+        """In a chain kernel the next group lays out shared memory
+        differently: the mbarriers of this body are invalidated first."""
+        w = self.pg.w
+        if not self.stage_nodes:
+            return
+        w.open("if (PM_CH)")
+        w("__syncthreads();")
+        w.open("if (threadIdx.x == 0)")
+        w("pm_mbar_inval(pm_bar);")
+        if self.prefetch:
+            w("pm_mbar_inval(pm_bar + 1);")
         w.close()
-        w("")
+        w.close()
 
     def gen_tile_setup(self, tile):
         """Descriptor, parameters, tile box, domains and region inference of
@@ -2296,7 +2330,7 @@ class StencilGen(object):
                                    "its domain and computed inline; it "
                                    "must be materialized" % f.name)
             else:
-                w("const %s %s = (%s) ? __ldg(b_%s + (%s)) : (%s)0;" % (
+                w("const %s %s = (%s) ? pm_ld<PM_CH>(b_%s + (%s)) : (%s)0;" % (
                     ctype(f.typ), t, guard, pg.fn(f),
                     pg.gindex(f, args, ctx, clamp_all=self.clamp),
                     ctype(f.typ)))
@@ -2327,7 +2361,7 @@ class StencilGen(object):
         else:
             if self.vec_stats is not None:
                 self.vec_stats[1] += 1      # a strided HBM read
-            w("const %s %s = __ldg(b_%s + (%s));" % (
+            w("const %s %s = pm_ld<PM_CH>(b_%s + (%s));" % (
                 ctype(f.typ), t, pg.fn(f),
                 pg.gindex(f, args, ctx, clamp_all=self.clamp)))
         ctx.define(key, t)
@@ -2468,7 +2502,7 @@ class StencilGen(object):
                 inb.append("c%d >= 0 && c%d <= d_%s_hi%d - d_%s_lo%d" % (
                     d, d, fnm, d, fnm, d))
                 coords.append("(long long)c%d * s_%s_%d" % (d, fnm, d))
-            w("sm_%s[i] = (%s) ? __ldg(b_%s + (%s)) : (%s)0;" % (
+            w("sm_%s[i] = (%s) ? pm_ld<PM_CH>(b_%s + (%s)) : (%s)0;" % (
                 nm, " && ".join(inb), fnm, " + ".join(coords),
                 ctype(n.func.typ)))
             w.close()
@@ -3850,6 +3884,224 @@ class ConstGen(object):
 
 
 # ---------------------------------------------------------------------------
+# ---------------------------------------------------------------------------
+# Chain kernels: consecutive small stencil groups in one launch
+CHAIN_DEFAULT_TILES = 512        # largest member group (tiles at estimates)
+CHAIN_PARAM_BYTES = 28000        # kernel parameter budget of one chain
+
+
+def _chain_limit(pipeline):
+    """Option ``chain`` (``'chain'``, ``'chain=N'`` or ``('chain', N)``):
+    runs of consecutive stencil groups of at most N tiles each (at the
+    parameter estimates) become one launch; None when off."""
+    v = _opt(pipeline, 'chain')
+    if v is not None:
+        return int(v)
+    return CHAIN_DEFAULT_TILES if 'chain' in pipeline.options else None
+
+
+def _launch_param_bytes(sg):
+    """Upper estimate of sizeof(<k>_launch): tensor maps, parameters,
+    buffer pointers, tile grid, launch fields."""
+    pg = sg.pg
+    na = sg.plan.anchor.ndims
+    desc = 128 * len(sg.stage_nodes) + 8 * (len(pg.params) + len(sg.bufs)) \
+        + 12 * na + 8 + 4 * len(sg.stage_nodes)
+    desc = (desc + 63) // 64 * 64
+    return desc + 64
+
+
+def plan_chains(pg, pipeline):
+    """Chains of launches: (member launch indices, phase of each member).
+
+    A member is a stencil group's launch whose tile count at the parameter
+    estimates is at most the option's limit (not prefetching, not launched
+    with programmatic serialization, same CTA size as the others); members
+    are consecutive in program order.  A member's phase is one more than
+    the latest earlier member it has a read-after-write, write-after-read
+    or write-after-write hazard with (0 without one): members of one phase
+    run concurrently, a grid barrier separates phases."""
+    limit = _chain_limit(pipeline)
+    if limit is None or 'pdl' in pipeline.options:
+        return []
+    from .grouping import _comp_sizes
+    sizes = _comp_sizes(pipeline)
+    comp_of = pipeline.func_map
+
+    def tiles(sg):
+        s = sizes.get(comp_of.get(sg.plan.anchor))
+        if s is None:
+            return None
+        return s / float(np.prod(sg.plan.tile))
+
+    runs, cur = [], []
+    for j in range(len(pg.launch_fns)):
+        sg = pg.stencil_of.get(j)
+        ok = sg is not None and not sg.prefetch and \
+            j not in pg.launch_main and tiles(sg) is not None and \
+            tiles(sg) <= limit
+        if ok and cur:
+            first = pg.stencil_of[cur[0]]
+            size = sum(_launch_param_bytes(pg.stencil_of[i]) for i in cur)
+            if sg.plan.threads != first.plan.threads or \
+                    sg.launch_bounds != first.launch_bounds or \
+                    size + _launch_param_bytes(sg) > CHAIN_PARAM_BYTES:
+                runs.append(cur)
+                cur = []
+        if ok:
+            cur.append(j)
+        else:
+            if cur:
+                runs.append(cur)
+            cur = []
+    if cur:
+        runs.append(cur)
+    chains = []
+    for run in runs:
+        if len(run) < 2:
+            continue
+        phase = {}
+        for j in run:
+            rj, wj = pg.launch_rw[j]
+            p = 0
+            for i in run:
+                if i >= j:
+                    break
+                ri, wi = pg.launch_rw[i]
+                if (wi & rj) or (ri & wj) or (wi & wj):
+                    p = max(p, phase[i] + 1)
+            phase[j] = p
+        chains.append((run, [phase[j] for j in run]))
+    return chains
+
+
+def gen_chains(pg, pipeline):
+    """Emit one kernel per chain (``pm_<name>_chain<c>``) that runs its
+    members' kernel bodies phase by phase, with a bounded grid barrier
+    (``pm_grid_sync``) between phases, and its host launcher; the chain
+    replaces its members in the launch list of the single-image entry
+    points (batches keep the per-group kernels).  The grid is the largest
+    phase's tile count, capped by the CTAs resident on the GPU at once, so
+    every CTA of the launch is on the GPU together."""
+    chains = plan_chains(pg, pipeline)
+    if not chains:
+        return
+    w = pg.w
+    w("// ---- chain kernels: consecutive small groups in one launch")
+    w("__device__ unsigned pm_chain_ctr[%d];   // grid-barrier counters" %
+      len(chains))
+    w("static unsigned* pm_chain_ctr_ptr[64];  // per device")
+    w.open("static unsigned* pm_chain_counters()")
+    w("const int dev = pm_cur_dev();")
+    w.open("if (!pm_chain_ctr_ptr[dev])")
+    w("void* p = nullptr;")
+    w("if (cudaGetSymbolAddress(&p, pm_chain_ctr) != cudaSuccess) return "
+      "nullptr;")
+    w("pm_chain_ctr_ptr[dev] = static_cast<unsigned*>(p);")
+    w.close()
+    w("return pm_chain_ctr_ptr[dev];")
+    w.close()
+    w("")
+    replace = {}
+    pg.meta['chains'] = []
+    for c, (run, phases) in enumerate(chains):
+        sgs = [pg.stencil_of[j] for j in run]
+        ck = "pm_%s_chain%d" % (pg.pname, c)
+        nt = sgs[0].plan.threads
+        smem = max(sg.plan.smem_bytes for sg in sgs)
+        nph = max(phases) + 1
+        w("// chain %d: %s in %d phases" % (
+            c, ", ".join("%s (phase %d)" % (sg.k, p)
+                         for sg, p in zip(sgs, phases)), nph))
+        w.open("struct %s_launch" % ck)
+        for m, sg in enumerate(sgs):
+            w("%s_launch m%d;" % (sg.k, m))
+        w("unsigned* ctr;        // grid-barrier counter, zeroed per launch")
+        w("int rot[%d];          // CTA of each member's first tile" %
+          len(sgs))
+        w.close("};")
+        w("static_assert(sizeof(%s_launch) <= 32000, \"chain parameters\");"
+          % ck)
+        w('extern "C" __global__ void __launch_bounds__(%s) %s(const '
+          '__grid_constant__ %s_launch C)' % (sgs[0].launch_bounds, ck, ck))
+        w.open("")
+        w("const int nb = (int)gridDim.x, b = (int)blockIdx.x;")
+        for p in range(nph):
+            if p:
+                w("if (!pm_grid_sync(C.ctr, %du * (unsigned)nb, "
+                  "&pm_err_word)) return;" % p)
+            w("// phase %d" % p)
+            for m, (sg, q) in enumerate(zip(sgs, phases)):
+                if q == p:
+                    w("%s_body<true>(C.m%d, (b + nb - C.rot[%d]) %% nb, nb);"
+                      % (sg.k, m, m))
+        w.close()
+        w("static bool %s_attr[64];     // per device" % ck)
+        w("static int %s_resident[64];  // per device" % ck)
+        w.open("static int launch_%s(pm_args& A, const size_t* wsoff, "
+               "cudaStream_t s)" % ck)
+        w("%s_launch C; memset(&C, 0, sizeof(C));" % ck)
+        w("long long nt = 0, ph[%d] = {0};" % nph)
+        w("int st = PM_OK;")
+        for m, (sg, q) in enumerate(zip(sgs, phases)):
+            w("if ((st = fill_%s(C.m%d.d0, A, wsoff, &nt))) return st;" % (
+                sg.k, m))
+            w("if (nt > 0x7fffffffLL) return PM_ERR_UNSUPPORTED;")
+            w("C.m%d.nimg = 1; C.m%d.total = (int)nt; C.m%d.stride = 1;" % (
+                m, m, m))
+            w("C.rot[%d] = (int)(ph[%d] & 0x7fffffff); ph[%d] += nt;" % (
+                m, q, q))
+        w("long long need = 0;")
+        w("for (int p = 0; p < %d; ++p) need = pm_llmax(need, ph[p]);" % nph)
+        w("if (need == 0) return PM_OK;")
+        w("const int dev = pm_cur_dev();")
+        w.open("if (!%s_attr[dev])" % ck)
+        w("if (cudaFuncSetAttribute(%s, cudaFuncAttributeMaxDynamicShared"
+          "MemorySize, %d) != cudaSuccess) return PM_ERR_CUDA;" % (ck, smem))
+        w("int per_sm = 0, sms = 0;")
+        w("if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, "
+          "dev) != cudaSuccess || cudaOccupancyMaxActiveBlocksPerMultiprocessor"
+          "(&per_sm, %s, %d, %d) != cudaSuccess || per_sm < 1) return "
+          "PM_ERR_CUDA;" % (ck, nt, smem))
+        w("%s_resident[dev] = per_sm * sms;" % ck)
+        w("%s_attr[dev] = true;" % ck)
+        w.close()
+        w("const long long grid = pm_llmin(need, %s_resident[dev]);" % ck)
+        w("for (int m = 0; m < %d; ++m) C.rot[m] = (int)(C.rot[m] %% grid);"
+          % len(sgs))
+        w("unsigned* ctr = pm_chain_counters();")
+        w("if (!ctr) return PM_ERR_CUDA;")
+        w("C.ctr = ctr + %d;" % c)
+        w("if (cudaMemsetAsync(C.ctr, 0, sizeof(unsigned), s) != cudaSuccess)"
+          " return PM_ERR_CUDA;")
+        w("%s<<<(unsigned)grid, %d, %d, s>>>(C);" % (ck, nt, smem))
+        w("return cudaGetLastError() == cudaSuccess ? PM_OK : PM_ERR_CUDA;")
+        w.close()
+        w("")
+        replace[run[0]] = ("launch_" + ck, run)
+        pg.meta['chains'].append({
+            'kernel': ck, 'members': [sg.k for sg in sgs],
+            'phases': phases, 'smem': smem, 'threads': nt})
+    # the chains take their members' places in the launch list
+    fns, rw, main = [], [], []
+    member = set(j for run, _ in chains for j in run)
+    for j in range(len(pg.launch_fns)):
+        if j in replace:
+            fn, run = replace[j]
+            reads, writes = set(), set()
+            for i in run:
+                reads |= pg.launch_rw[i][0]
+                writes |= pg.launch_rw[i][1]
+            fns.append(fn)
+            rw.append((reads, writes))
+        elif j not in member:
+            if j in pg.launch_main:
+                main.append(len(fns))
+            fns.append(pg.launch_fns[j])
+            rw.append(pg.launch_rw[j])
+    pg.launch_fns, pg.launch_rw, pg.launch_main = fns, rw, main
+
+
 def generate_code_for_pipeline(pipeline):
     pg = PipelineGen(pipeline)
     pg.slot_of = getattr(pipeline, '_storage_assign', {})
@@ -3868,13 +4120,16 @@ def generate_code_for_pipeline(pipeline):
     # generate groups into `body` first so helper declarations can precede
     pg.launch_rw = []
     pg.launch_main = []
+    pg.stencil_of = {}
     pg.conc_streams = 0
     pg.conc_events = 0
     for g in pipeline.groups:
         plan = g.plan
         n0 = len(pg.launch_fns)
         if plan.kind == 'stencil':
-            StencilGen(pg, g).generate()
+            sg = StencilGen(pg, g)
+            sg.generate()
+            pg.stencil_of[n0] = sg
         elif plan.kind == 'reduction':
             ReductionGen(pg, g).generate()
         else:
@@ -3886,6 +4141,15 @@ def generate_code_for_pipeline(pipeline):
             raise CodegenError("group %s: expected one launch" % (
                 [c.func.name for c in g.comps],))
         pg.launch_rw.append(pg.group_rw(g))
+    pg.group_launch_rw = list(pg.launch_rw)
+    pg.group_launch_main = list(pg.launch_main)
+    gen_chains(pg, pipeline)
+    # kernel launches of one single-image call (a Reduction: its init
+    # and accumulation; a chain: one for all its members)
+    pg.meta['launches'] = sum(
+        {'stencil': 1, 'reduction': 2}.get(g.plan.kind, 0)
+        for g in pipeline.groups) - sum(
+            len(ch['members']) - 1 for ch in pg.meta.get('chains', []))
     pg.w = pg_w
     w = pg.w
     w("// pipeline %s -- generated by polymage_b200 for sm_100a" %

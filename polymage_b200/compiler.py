@@ -17,12 +17,25 @@ as ``"name=value"`` strings or ``(name, value)`` tuples:
   memory), ``tight_stage`` (no TMA slack for narrow whole innermost
   dimensions), ``no_privatize`` (reductions accumulate straight into
   HBM), ``no_storage_reuse``;
+* grouping beyond the reference's: ``fuse_all`` (every non-const stage in
+  one group when legal), ``('merge_small', N)`` (a group merges into its
+  only child when both have stages of at most N points);
+* staging and tiling: ``stage_pointwise`` (inputs read at one offset are
+  staged too), ``prefetch`` (a CTA loads its next tile while computing
+  this one), ``channel_tile`` (a small leading channel dimension tiled
+  whole), ``oob_zero`` (reads outside a producer's domain read 0),
+  ``no_row_pad``, ``no_tile_shrink``;
+* reductions: ``red_unroll=N``, ``red_spread``, ``no_gather`` (scatter
+  form instead of output-stationary);
 * launches: ``streams=N`` (concurrent streams for independent groups, 1
-  for the caller's stream only);
+  for the caller's stream only), ``pdl`` (programmatic stream
+  serialization), ``chain`` / ``('chain', N)`` (consecutive stencil groups
+  of at most N tiles each as phases of one launch, grid barriers between
+  dependent phases);
 * switches of single optimisations, for measurement and debugging:
   ``no_inside`` (every tile on the general path), ``guarded`` (one point
-  per iteration), ``no_vec``, ``no_cblock``, ``no_static_res``,
-  ``no_fold_clamps``.
+  per iteration), ``no_vec``, ``no_vec2``, ``no_cblock``,
+  ``no_static_res``, ``no_fold_clamps``.
 """
 
 from .pipe import Pipeline

@@ -29,9 +29,15 @@
 #define PM_KERR_TMA_TIMEOUT 1u
 #define PM_KERR_REGION 2u
 #define PM_KERR_QUEUE 4u
+#define PM_KERR_GRID_TIMEOUT 8u
 
 #ifndef PM_WAIT_LIMIT
 #define PM_WAIT_LIMIT (1 << 24)
+#endif
+// polls of a grid barrier (each after a ~128 ns sleep) before it gives up:
+// well above the longest kernel that can hold SMs the barrier's CTAs wait for
+#ifndef PM_GRID_WAIT_LIMIT
+#define PM_GRID_WAIT_LIMIT (1 << 21)
 #endif
 
 // ---------------------------------------------------------------------------
@@ -75,6 +81,69 @@ __device__ __forceinline__ void pm_fence_barrier_init() {
 // async-proxy (TMA) writes to the same bytes
 __device__ __forceinline__ void pm_fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// An mbarrier's bytes must be invalidated before they are used for
+// anything else (another barrier, staged data of another group).
+__device__ __forceinline__ void pm_mbar_inval(uint64_t* bar) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(pm_smem_addr(bar))
+               : "memory");
+}
+
+// Global loads of a group's kernel body.  A standalone launch reads through
+// the read-only (non-coherent) path: nothing it reads is written while it
+// runs.  A body inside a chain kernel (several groups, one launch, grid
+// barriers between dependent groups) reads data that other CTAs of the same
+// launch wrote before the last barrier, so it bypasses L1 (ld.global.cg).
+template <bool CH, typename T>
+__device__ __forceinline__ T pm_ld(const T* p) {
+  if constexpr (CH) return __ldcg(p);
+  else return __ldg(p);
+}
+
+// Between two phases of a chain kernel: every generic-proxy access of this
+// thread (global stores read by later TMA loads, shared memory that a later
+// group's TMA overwrites) is ordered before later async-proxy accesses.
+__device__ __forceinline__ void pm_fence_proxy_async_all() {
+  asm volatile("fence.proxy.async;" ::: "memory");
+}
+
+__device__ __forceinline__ unsigned pm_ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(p)
+               : "memory");
+  return v;
+}
+
+// Grid-wide barrier of a chain kernel: every CTA arrives on the launch's
+// counter (zeroed before the launch) and waits until `target` arrivals
+// (gridDim.x times the barrier's ordinal) are counted.  The wait is bounded:
+// when it runs out the error word records PM_KERR_GRID_TIMEOUT and every
+// thread gets false, so the kernel returns instead of spinning forever.
+// The CTAs of a chain launch all fit on the GPU at once (the grid is capped
+// by the occupancy calculator), so the wait ends once any concurrently
+// running kernel that holds SMs has finished.
+__device__ __forceinline__ bool pm_grid_sync(unsigned* ctr, unsigned target,
+                                             unsigned* err) {
+  pm_fence_proxy_async_all();
+  __syncthreads();
+  int ok = 1;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(ctr, 1u);
+    int it = 0;
+    while (pm_ld_acquire(ctr) < target) {
+      if (++it > PM_GRID_WAIT_LIMIT) {
+        atomicOr(err, PM_KERR_GRID_TIMEOUT);
+        ok = 0;
+        break;
+      }
+      __nanosleep(128);
+    }
+    __threadfence();
+    pm_fence_proxy_async_all();
+  }
+  return __syncthreads_and(ok) != 0;
 }
 
 // Programmatic dependent launch: a kernel launched with programmatic

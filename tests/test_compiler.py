@@ -397,7 +397,7 @@ def test_tight_staging_of_interleaved_channels():
     for opts in (('rblock=8',), ('rblock=8', 'tight_stage')):
         p = build_laplacian(rows=270, cols=480, options=opts)
         src = p.generate_code().source
-        seg = src[src.index('pm_laplacian_g0(const'):]
+        seg = src[src.index('pm_laplacian_g0_body(const'):]
         seg = seg[:seg.index('// stage')]
         loops[len(opts)] = int(re.findall(
             r'for \(int i = threadIdx.x; i < (\d+);', seg)[0])
