@@ -36,7 +36,14 @@ round trip it saves.  The Jacobi steps, the 2-D multigrid cycles and NAS MG
 also stage their pointwise-read right-hand sides by TMA (option
 stage_pointwise: Jacobi 2-D 0.116 vs 0.132 ms, 3-D 0.154 vs 0.165 ms,
 V-cycle 0.073 vs 0.083 ms, W-cycle 0.138 vs 0.155 ms, NAS MG 0.255 vs
-0.264 ms; the 3-D cycles are slower with it)."""
+0.264 ms; the 3-D cycles are slower with it).
+A later sweep of the CTA-shape knobs (same timing, one box): the camera
+pipe with 3 resident CTAs asked of ptxas (0.0491 vs 0.0553 ms), the L=4
+pyramid with 4 rows per thread and its tile regions computed by one
+thread (option shared_regions: 0.1735 vs 0.1875 ms; every other pipeline
+is slower with that option), the L=8 pyramid and the local Laplacian with
+4 rows per thread (0.2164 vs 0.2237 ms, 0.1474 vs 0.1496 ms),
+interpolation with 3 resident CTAs (0.3048 vs 0.3138 ms)."""
 
 import functools
 
@@ -58,21 +65,22 @@ HARRIS = dict(tile_sizes=(32, 64), group_size=11,
 UNSHARP = dict(tile_sizes=(64, 128), group_size=10,
                options=('rblock=16', 'inline_budget=400', 'threads=128'))
 CAMPIPE = dict(tile_sizes=(32, 128), group_size=12,
-               options=('rblock=4', 'fuse_all', 'channel_tile'))
+               options=('rblock=4', 'fuse_all', 'channel_tile',
+                        'min_blocks=3'))
 BILATERAL = dict(tile_sizes=(1, 32, 128), group_size=10,
                  options=(('red_tile', (16, 256)), 'rblock=4',
                           'stage_pointwise'))
 PYRAMID = dict(tile_sizes=(32, 64), group_size=10,
-               options=('rblock=8', 'min_blocks=4'))
+               options=('rblock=4', 'min_blocks=4', 'shared_regions'))
 # 8 levels, indices clamped at every level's borders (any image size)
 PYRAMID8 = dict(L=8, tile_sizes=(32, 64), group_size=10,
-                options=('rblock=8', 'min_blocks=4'))
+                options=('rblock=4', 'min_blocks=4'))
 
 # local Laplacian filter (the video demo's pipeline_laplacian), 1080p frames
 # (option tight_stage: the uint8 [x][y][3] frame is staged without the TMA
 # alignment slack of its 3-byte innermost rows, 0.148 vs 0.213 ms)
 LAPLACIAN = dict(tile_sizes=(32, 64), group_size=10,
-                 options=('rblock=8', 'tight_stage'))
+                 options=('rblock=4', 'tight_stage'))
 
 # The widening pipelines at the reference Makefiles' settings: Jacobi 2-D
 # N=2048 and 3-D N=128 with 10 steps each (stencil/jacobi{2D,3D}/
@@ -80,7 +88,8 @@ LAPLACIAN = dict(tile_sizes=(32, 64), group_size=10,
 # grid, 10 pre-smoothings and none after or on the coarsest level
 # (multigrid/jacobi{2D,3D}/Makefile:10-16), NAS MG class W (NAS-PB-MG-3.2/
 # Makefile:9), interpolation of a 2048x2048 RGBA image.
-INTERPOLATE = dict(rows=2048, cols=2048, tile_sizes=(32, 64), group_size=11)
+INTERPOLATE = dict(rows=2048, cols=2048, tile_sizes=(32, 64), group_size=11,
+                   options=('min_blocks=3',))
 JACOBI2D = dict(N=2048, T=10, tile_sizes=(32, 64), group_size=5,
                 options=('stage_pointwise',))
 JACOBI3D = dict(N=128, T=10, tile_sizes=(8, 16, 32), group_size=1,

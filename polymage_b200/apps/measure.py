@@ -384,6 +384,8 @@ def main():
     ap.add_argument("--options", default=None,
                     help="JSON list of options added to the catalog build "
                          "(e.g. '[\"chain\"]')")
+    ap.add_argument("--drop-options", default=None,
+                    help="JSON list of catalog options left out")
     args = ap.parse_args()
     if args.int_peak:
         print(json.dumps(int_peak()))
@@ -398,13 +400,16 @@ def main():
             print(json.dumps(measure_host(app, min(args.steps, 20))))
         else:
             cp = None
-            if args.options:
-                opts = [tuple(o) if isinstance(o, list) else o
-                        for o in json.loads(args.options)]
-                cp = catalog.variant(app, opts).build()
+            add = [tuple(o) if isinstance(o, list) else o
+                   for o in json.loads(args.options or "[]")]
+            drop = [tuple(o) if isinstance(o, list) else o
+                    for o in json.loads(args.drop_options or "[]")]
+            if add or drop:
+                cp = catalog.variant(app, add, drop).build()
             r = measure(app, args.steps, args.warmup, warm=args.warm, cp=cp)
-            if args.options:
-                r["options"] = json.loads(args.options)
+            if add or drop:
+                r["options"] = add
+                r["dropped"] = drop
             print(json.dumps(r))
 
 

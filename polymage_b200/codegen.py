@@ -513,6 +513,36 @@ def _inner_parity(f, var):
     return False
 
 
+def _top_level_decls(lines):
+    """(type, name) of the ``int`` / ``bool`` variables that generated
+    statements declare outside any braces, in order (declarator lists are
+    split at commas outside parentheses)."""
+    out = []
+    depth = 0
+    for raw in lines:
+        s = raw.strip()
+        if depth == 0:
+            m = re.match(r'(?:const )?(int|bool) (.*);$', s)
+            if m:
+                typ, rest = m.group(1), m.group(2)
+                par, cur, parts = 0, [], []
+                for ch in rest:
+                    if ch == '(':
+                        par += 1
+                    elif ch == ')':
+                        par -= 1
+                    if ch == ',' and par == 0:
+                        parts.append("".join(cur))
+                        cur = []
+                    else:
+                        cur.append(ch)
+                parts.append("".join(cur))
+                for p in parts:
+                    out.append((typ, p.split('=')[0].strip()))
+        depth += s.count('{') - s.count('}')
+    return out
+
+
 def _opt(pipeline, name, default=None):
     from .tiling import _option
     return _option(pipeline, name, default)
@@ -1995,8 +2025,36 @@ class StencilGen(object):
         for f in self.bufs:
             if f not in plan.node_of:
                 pg.declare_domain(w, f, ctx, True)
-        # region inference
-        self.gen_regions()
+        # region inference: the same values for every thread of the CTA.
+        # By default every thread computes them (a few hundred integer
+        # instructions for a group of many stages); with option
+        # 'shared_regions' thread 0 computes them and hands them to the
+        # others through shared memory, at the cost of a CTA barrier and
+        # the single thread's latency (faster only for the L=4 pyramid)
+        if 'shared_regions' not in pg.p.options:
+            self.gen_regions()
+            return
+        tmp = W()
+        tmp.ind = w.ind + 1
+        pg.w = ctx.w = tmp
+        try:
+            self.gen_regions()
+        finally:
+            pg.w = ctx.w = w
+        names = _top_level_decls(tmp.lines)
+        self.nshared = getattr(self, 'nshared', 0) + 1
+        arr = "pm_ts%d" % self.nshared
+        w("__shared__ int %s[%d];   // this tile's regions" % (arr,
+                                                             len(names)))
+        w.open("if (threadIdx.x == 0)")
+        w.lines.extend(tmp.lines)
+        for i, (typ, nm) in enumerate(names):
+            w("%s[%d] = (int)%s;" % (arr, i, nm))
+        w.close()
+        w("__syncthreads();")
+        for i, (typ, nm) in enumerate(names):
+            w("const %s %s = %s%s[%d];" % (
+                typ, nm, "(bool)" if typ == "bool" else "", arr, i))
 
     def gen_buffers(self, buf):
         """HBM buffer pointers and shared-memory buffers of the current

@@ -33,9 +33,10 @@ as ``"name=value"`` strings or ``(name, value)`` tuples:
   of at most N tiles each as phases of one launch, grid barriers between
   dependent phases);
 * switches of single optimisations, for measurement and debugging:
-  ``no_inside`` (every tile on the general path), ``guarded`` (one point
-  per iteration), ``no_vec``, ``no_vec2``, ``no_cblock``,
-  ``no_static_res``, ``no_fold_clamps``.
+  ``shared_regions`` (one thread computes a tile's regions and shares
+  them through shared memory), ``no_inside`` (every tile on the general
+  path), ``guarded`` (one point per iteration), ``no_vec``, ``no_vec2``,
+  ``no_cblock``, ``no_static_res``, ``no_fold_clamps``.
 """
 
 from .pipe import Pipeline

@@ -482,3 +482,31 @@ def test_whole_channel_tiles_fold_channel_conditions():
     fast = fast[:fast.index("\n      }\n      else")]
     assert "== 2)" not in fast and "== 1)" not in fast
     assert fast.count("b_process[gb") == fast.count("b_process[")
+
+
+def test_shared_regions_broadcast_every_declared_region():
+    """Option 'shared_regions': thread 0 computes the tile's regions and
+    the interior flag, every value the per-thread form declares at the
+    top level is stored and read back under the same name and type."""
+    from polymage_b200.codegen import _top_level_decls
+    decls = _top_level_decls([
+        "const int r_a_lo0 = pm_imax(a_lo0, d_a_lo0), r_a_hi0 = x;",
+        "int r_b_lo0 = 0x3fffffff, r_b_hi0 = -0x3fffffff;",
+        "if (!(e)) {",
+        "  { const int ea = 1, eb = 2; r_b_lo0 = pm_imin(r_b_lo0, ea); }",
+        "}",
+        "int o_c_lo0 = (t0 == 0) ? pm_imax(a_lo0, d_c_lo0) : 5;",
+        "const bool pm_inside = r_a_lo0 >= 0 && (r_b_hi0 <= 3);"])
+    assert decls == [("int", "r_a_lo0"), ("int", "r_a_hi0"),
+                     ("int", "r_b_lo0"), ("int", "r_b_hi0"),
+                     ("int", "o_c_lo0"), ("bool", "pm_inside")]
+    from polymage_b200.apps import catalog
+    src = catalog.variant("harris", ("shared_regions",)).generate_code() \
+        .source
+    body = src[src.index("pm_harris_g0_body(const"):]
+    body = body[:body.index("// stage")]
+    assert "__shared__ int pm_ts1[" in body
+    assert "if (threadIdx.x == 0) {" in body
+    assert "const bool pm_inside = (bool)pm_ts1[" in body
+    plain = catalog.variant("harris").generate_code().source
+    assert "pm_ts1" not in plain
