@@ -43,7 +43,9 @@ pyramid with 4 rows per thread and its tile regions computed by one
 thread (option shared_regions: 0.1735 vs 0.1875 ms; every other pipeline
 is slower with that option), the L=8 pyramid and the local Laplacian with
 4 rows per thread (0.2164 vs 0.2237 ms, 0.1474 vs 0.1496 ms),
-interpolation with 3 resident CTAs (0.3048 vs 0.3138 ms)."""
+interpolation with 3 resident CTAs (0.3048 vs 0.3138 ms).  Harris sums
+its 3x3 box sums and Sobel taps as row sums that the rows of a thread's
+block share (option separable: 0.0255 vs 0.0274 ms)."""
 
 import functools
 
@@ -61,7 +63,8 @@ from .nlmeans import build_nlmeans
 from .max_filter import build_maxfilter
 
 HARRIS = dict(tile_sizes=(32, 64), group_size=11,
-              options=('rblock=8', 'min_blocks=4', 'threads=128'))
+              options=('rblock=8', 'min_blocks=4', 'threads=128',
+                       'separable'))
 UNSHARP = dict(tile_sizes=(64, 128), group_size=10,
                options=('rblock=16', 'inline_budget=400', 'threads=128'))
 CAMPIPE = dict(tile_sizes=(32, 128), group_size=12,
@@ -150,8 +153,12 @@ def build(name):
 def variant(name, extra_options=(), drop_options=()):
     """The uncompiled pipeline of a shipped build with options added
     (``extra_options``) or removed (``drop_options``)."""
+    import inspect
     b, kw = _BUILDERS[name]
     kw = dict(kw)
-    opts = [o for o in kw.get('options', ()) if o not in drop_options]
+    base = kw.get('options')
+    if base is None:
+        base = inspect.signature(b).parameters['options'].default
+    opts = [o for o in base if o not in drop_options]
     kw['options'] = tuple(opts) + tuple(extra_options)
     return b(**kw)

@@ -17,6 +17,9 @@ as ``"name=value"`` strings or ``(name, value)`` tuples:
   memory), ``tight_stage`` (no TMA slack for narrow whole innermost
   dimensions), ``no_privatize`` (reductions accumulate straight into
   HBM), ``no_storage_reuse``;
+* expressions: ``separable`` (rank-one rectangular weighted sums of one
+  producer, at least six terms, summed as row sums: polymage_b200/
+  separable.py);
 * grouping beyond the reference's: ``fuse_all`` (every non-const stage in
   one group when legal), ``('merge_small', N)`` (a group merges into its
   only child when both have stages of at most N points);

@@ -317,6 +317,9 @@ class Pipeline(object):
         # the passes, in the reference's order
         bounds.bounds_check_pass(self)
         inline.inline_pass(self)
+        if 'separable' in self._options:
+            from .separable import separable_pass
+            self._separable = separable_pass(self)
         self._groups = [Group([c]) for c in self._comps]
         self._refresh_groups()
         if self._grouping:
