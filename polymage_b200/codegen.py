@@ -3405,10 +3405,14 @@ class ReductionGen(object):
         else:
             StencilGen.decompose(self, "i", plan.tile, "j")
         lv = _loop_vars(nr)
+        # A point past the tile's last one (a partial tile) is clamped onto
+        # it and only its accumulation is skipped: its reads stay in
+        # bounds and need no branch, so the unrolled iterations' loads can
+        # all be issued before the first atomic
+        w("const bool pm_pt = !(%s);" % " || ".join(
+            "a_lo%d + j%d > a_hi%d" % (d, d, d) for d in range(nr)))
         for d in range(nr):
-            w("const int q%d = a_lo%d + j%d;" % (d, d, d))
-        w("if (%s) continue;" % " || ".join("q%d > a_hi%d" % (d, d)
-                                           for d in range(nr)))
+            w("const int q%d = pm_imin(a_lo%d + j%d, a_hi%d);" % (d, d, d, d))
         rbind = dict(zip(rvars, lv))
         saved_lo = dict(ctx.var_lo)
         for d, dom in enumerate(f.reductionDomain):
@@ -3438,7 +3442,7 @@ class ReductionGen(object):
                 if is_data_dependent(tgt[d])) or "true"
             cc = ctx.cond(cond, tbind) if cond is not None else "true"
             val = ctx.expr(expr, rbind) if shared else None
-            w.open("if ((%s) && (%s))" % (inb, cc))
+            w.open("if (pm_pt && (%s) && (%s))" % (inb, cc))
             if val is None:
                 val = ctx.expr(expr, rbind)
             if priv:
