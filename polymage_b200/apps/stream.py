@@ -64,16 +64,22 @@ def _request_io(kind, r, c, dev, gen):
             {'blend': torch.empty((3, r, c), device=dev)})
 
 
-def serve(reqs, device=None, budget=8 << 30, seed=1, keep=False):
+def serve(reqs, device=None, budget=8 << 30, seed=1, keep=False,
+          concurrent=True):
     """Run the stream; returns totals (GPU ms of the batch calls, output
     pixels, compulsory bytes, chunks, batch calls); with ``keep`` also
-    every request's (pipeline, params, inputs, outputs)."""
+    every request's (pipeline, params, inputs, outputs).  ``concurrent``:
+    the pipelines' batch calls of a chunk run on their own streams, forked
+    from the timing stream and joined back into it (they share no data:
+    each library has its own workspace); otherwise one after another on
+    the timing stream."""
     import torch
     dev = device or torch.device("cuda", torch.cuda.current_device())
     libs = dict((k, catalog.build(k)) for k in KINDS)
     gen = torch.Generator(device=dev)
     gen.manual_seed(seed)
     stream = torch.cuda.current_stream(dev)
+    side = dict((k, torch.cuda.Stream(dev)) for k in KINDS)
     total_ms, pixels, nbytes, chunks, calls = 0.0, 0, 0, 0, 0
     kept = []
     i = 0
@@ -102,9 +108,16 @@ def serve(reqs, device=None, budget=8 << 30, seed=1, keep=False):
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for kind in KINDS:
-            if per[kind][0]:
-                libs[kind].run_batch(*per[kind], stream=stream.cuda_stream)
-                calls += 1
+            if not per[kind][0]:
+                continue
+            s = stream
+            if concurrent:
+                s = side[kind]
+                s.wait_event(e0)
+            libs[kind].run_batch(*per[kind], stream=s.cuda_stream)
+            if concurrent:
+                stream.wait_stream(s)
+            calls += 1
         e1.record(stream)
         torch.cuda.synchronize(dev)
         for cp in libs.values():
@@ -124,9 +137,14 @@ def main():
     ap.add_argument("--requests", type=int, default=1024)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--budget-gb", type=float, default=8.0)
+    ap.add_argument("--serial", action="store_true",
+                    help="the pipelines' batches one after another")
     args = ap.parse_args()
     reqs = make_stream(args.requests, args.seed)
-    r = serve(reqs, budget=int(args.budget_gb * (1 << 30)), seed=args.seed)
+    serve(reqs, budget=int(args.budget_gb * (1 << 30)), seed=args.seed,
+          concurrent=not args.serial)      # sizes workspaces
+    r = serve(reqs, budget=int(args.budget_gb * (1 << 30)), seed=args.seed,
+              concurrent=not args.serial)
     r["mpix_s"] = r["pixels"] / (r["ms"] / 1e3) / 1e6
     r["gb_s"] = r["bytes"] / (r["ms"] / 1e3) / 1e9
     print(json.dumps(r))
