@@ -4052,7 +4052,9 @@ def gen_chains(pg, pipeline):
     w("// ---- chain kernels: consecutive small groups in one launch")
     w("__device__ unsigned pm_chain_ctr[%d];   // grid-barrier counters" %
       len(chains))
-    w("static unsigned* pm_chain_ctr_ptr[64];  // per device")
+    w("// per device: the counters' address, looked up on the first chain")
+    w("// launch (cudaDeviceReset reloads the module and invalidates it)")
+    w("static unsigned* pm_chain_ctr_ptr[64];")
     w.open("static unsigned* pm_chain_counters()")
     w("const int dev = pm_cur_dev();")
     w.open("if (!pm_chain_ctr_ptr[dev])")
