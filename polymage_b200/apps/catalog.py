@@ -111,8 +111,13 @@ NLMEANS = dict(rows=256, cols=256)
 # max filter (radius 26) on a 1536x2560 landscape image: the spec's
 # vert_log rows are [26, C-R-79], non-empty only when C > R + 104
 # (tiles of 8 x 32 pixels x 3 channels for its reductions)
+# (its vert_log and vert arrays are stored slice-outermost, so that the
+# final maximum's gather, whose warp spans channels and columns at one
+# slice, reads contiguous words: 1.137 vs 1.388 ms)
 MAXFILTER = dict(rows=1536, cols=2560,
-                 options=('oob_zero', ('red_tile', (8, 32, 3, 16))))
+                 options=('oob_zero', ('red_tile', (8, 32, 3, 16)),
+                          ('storage_order', (('vert', (3, 0, 1, 2)),
+                                             ('vert_log', (3, 0, 1, 2))))))
 
 _BUILDERS = {
     "harris": (build_harris, HARRIS),

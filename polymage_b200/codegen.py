@@ -746,16 +746,39 @@ class PipelineGen(object):
             w("const %s %s = %s.%s;" % (self.ptype(prm), self.pmap[prm], src,
                                         self.pmap[prm]))
 
+    def storage_perm(self, f):
+        """Dimensions of an intermediate array, outermost to innermost in
+        memory, when option ``('storage_order', ((name, dims), ...))``
+        reorders it (a gather that varies another dimension across a
+        warp then reads contiguous words); None for the domain's order.
+        Caller-owned inputs and outputs and const tables keep theirs."""
+        v = _opt(self.p, 'storage_order')
+        if not v or any(f is x for x in self.inputs + self.outputs) or \
+                getattr(f, 'is_const_func', False):
+            return None
+        for name, dims in v:
+            if name != f.name:
+                continue
+            dims = tuple(int(d) for d in dims)
+            if sorted(dims) != list(range(len(f.domain))):
+                raise CodegenError("storage_order of %s: %r is not a "
+                                   "permutation of its %d dimensions" % (
+                                       f.name, dims, len(f.domain)))
+            return None if dims == tuple(range(len(f.domain))) else dims
+        return None
+
     def row_pitch(self, f):
         """Elements the innermost rows of ``f`` are padded to a multiple
         of in memory: 16 bytes' worth for an intermediate array of two or
         more dimensions in the workspace (so that its rows are 16-byte
         aligned and TMA can stage it), 1 for caller-owned inputs and
-        outputs and for const tables, which are dense."""
+        outputs, for const tables, which are dense, and for reordered
+        intermediates (never staged by TMA)."""
         if any(f is x for x in self.inputs + self.outputs) or \
                 getattr(f, 'is_const_func', False) or \
                 len(f.domain) < 2 or f.typ.size() >= 16 or \
-                'no_row_pad' in self.p.options:
+                'no_row_pad' in self.p.options or \
+                self.storage_perm(f) is not None:
             return 1
         return 16 // f.typ.size()
 
@@ -765,7 +788,15 @@ class PipelineGen(object):
         for d, (lo, hi) in enumerate(dom):
             w("const int d_%s_lo%d = %s, d_%s_hi%d = %s;" % (n, d, lo, n, d,
                                                             hi))
-        if need_strides:
+        perm = self.storage_perm(f) if need_strides else None
+        if perm is not None:
+            # reordered: the strides follow the memory order ``perm``
+            w("const long long s_%s_%d = 1;" % (n, perm[-1]))
+            for j in range(len(perm) - 2, -1, -1):
+                d, dn = perm[j], perm[j + 1]
+                w("const long long s_%s_%d = s_%s_%d * (long long)(d_%s_hi%d"
+                  " - d_%s_lo%d + 1);" % (n, d, n, dn, n, dn, n, dn))
+        elif need_strides:
             nd = len(dom)
             pitch = self.row_pitch(f)
             w("const long long s_%s_%d = 1;" % (n, nd - 1))
@@ -785,11 +816,14 @@ class PipelineGen(object):
         n = self.fn(f)
         terms = []
         nd = len(args)
+        # the innermost dimension has stride 1 unless the array is
+        # reordered in memory (option storage_order)
+        unit = self.storage_perm(f) is None
         for d, a in enumerate(args):
             s = ctx.index(a)
             if clamp_all or (clamp_dd and is_data_dependent(a)):
                 s = "pm_clampi(%s, d_%s_lo%d, d_%s_hi%d)" % (s, n, d, n, d)
-            if d == nd - 1:
+            if d == nd - 1 and unit:
                 terms.append("(long long)(%s - d_%s_lo%d)" % (s, n, d))
             else:
                 terms.append("(long long)(%s - d_%s_lo%d) * s_%s_%d" % (
@@ -2952,7 +2986,7 @@ class StencilGen(object):
         # checked at run time
         vst = None
         if V == 4 and n.role == 'out' and n.func is plan.anchor and \
-                f.typ.size() == 4:
+                f.typ.size() == 4 and pg.storage_perm(f) is None:
             dlo = _const_int(f.domain[-1].lowerBound)
             if dlo is not None and (self._loop_res[f] - dlo) % 4 == 0:
                 vst = {'float': 'float4', 'int': 'int4'}.get(ctype(f.typ))
@@ -3007,7 +3041,9 @@ class StencilGen(object):
                             terms.append("%d * s_%s_%d" % (k, fnm, nd - 2))
                         if c:
                             terms.append("%d * s_%s_0" % (c, fnm))
-                        if u:
+                        if u and pg.storage_perm(f) is not None:
+                            terms.append("%d * s_%s_%d" % (u, fnm, nd - 1))
+                        elif u:
                             terms.append("%d" % u)
                         gidx = " + ".join(terms)
                     self._store(f, n, qs, v, flag, idx, gidx,
@@ -3083,6 +3119,10 @@ class StencilGen(object):
             w("{ long long dims[%d] = {%s}; int box[%d] = {%s};" % (
                 nd, dims, nd, box))
             pitch = pg.row_pitch(f)
+            if pg.storage_perm(f) is not None:
+                # a reordered array is staged by cooperative loads
+                w("  D.tma_%s = 0; (void)dims; (void)box; }" % nm)
+                continue
             w("  D.tma_%s = pm_use_tma() && pm_make_tmap(&D.tm_%s, D.b_%s, "
               "%d, dims, box, %d, %d, %s); }" % (
                   nm, nm, pg.fn(f), nd, f.typ.size(),

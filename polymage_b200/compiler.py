@@ -27,7 +27,9 @@ as ``"name=value"`` strings or ``(name, value)`` tuples:
   staged too), ``prefetch`` (a CTA loads its next tile while computing
   this one), ``channel_tile`` (a small leading channel dimension tiled
   whole), ``oob_zero`` (reads outside a producer's domain read 0),
-  ``no_row_pad``, ``no_tile_shrink``;
+  ``no_row_pad``, ``no_tile_shrink``, ``('storage_order', ((name,
+  dims), ...))`` (an intermediate array's dimensions, outermost to
+  innermost in memory);
 * reductions: ``red_unroll=N``, ``red_spread``, ``no_gather`` (scatter
   form instead of output-stationary);
 * launches: ``streams=N`` (concurrent streams for independent groups, 1

@@ -510,3 +510,32 @@ def test_shared_regions_broadcast_every_declared_region():
     assert "const bool pm_inside = (bool)pm_ts1[" in body
     plain = catalog.variant("harris").generate_code().source
     assert "pm_ts1" not in plain
+
+
+def test_storage_order_reorders_strides_only_of_intermediates():
+    """Option storage_order: the named intermediate's strides follow the
+    given memory order (innermost stride 1), every read of it multiplies
+    its innermost index by its stride, it is not staged by TMA, and an
+    invalid order is refused."""
+    import re
+    import pytest
+    from polymage_b200.apps import catalog
+    from polymage_b200.codegen import CodegenError
+    p = catalog.variant("maxfilter")
+    src = p.generate_code().source
+    st = dict(re.findall(r'const long long (s_vert_\d) = ([^;]*);', src))
+    assert st['s_vert_2'] == '1'
+    assert st['s_vert_1'].startswith('s_vert_2 *')
+    assert st['s_vert_0'].startswith('s_vert_1 *')
+    assert st['s_vert_3'].startswith('s_vert_0 *')
+    # the final maximum reads vert with a stride on its last index
+    assert re.search(r'b_vert \+ \(\(long long\)\([^;]*\) \* s_vert_3\)', src)
+    assert 'D.tma_vert = pm_use_tma()' not in src
+    # the caller's output keeps the domain order
+    assert 'const long long s_final_2 = 1;' in src
+    order = [o for o in catalog.MAXFILTER['options']
+             if isinstance(o, tuple) and o[0] == 'storage_order']
+    bad = catalog.variant("maxfilter", [('storage_order',
+                                         (('vert', (0, 1, 1, 2)),))], order)
+    with pytest.raises(CodegenError):
+        bad.generate_code()
