@@ -31,9 +31,13 @@ WIDENING = ("interpolate", "jacobi2d", "jacobi3d", "vcycle", "wcycle",
 FLUSH_BYTES = 256 << 20
 
 
-def workload(app, seed=0):
-    """(params, host inputs, output shapes/dtypes, pixels, description)."""
+def workload(app, seed=0, size=None):
+    """(params, host inputs, output shapes/dtypes, pixels, description).
+    ``size``: (rows, cols) instead of the benchmark size (max filter only,
+    for small profiling runs)."""
     rng = np.random.default_rng(seed)
+    if size is not None and app != 'maxfilter':
+        raise ValueError("a size can be given for the max filter only")
     if app == 'harris':
         n = 2048
         return ({'R': n - 2, 'C': n - 2},
@@ -127,7 +131,7 @@ def workload(app, seed=0):
                 n ** 3, "NAS MG mg3P class %s (%d^3) float64"
                 % (catalog.MG3P['prob_class'], n))
     if app == 'maxfilter':
-        R, C = catalog.MAXFILTER['rows'], catalog.MAXFILTER['cols']
+        R, C = size or (catalog.MAXFILTER['rows'], catalog.MAXFILTER['cols'])
         return ({'R': R, 'C': C},
                 {'img': rng.integers(0, 256, (3, R, C)).astype(np.float32)},
                 {'final': ((R, C, 3), np.int32)}, R * C,
@@ -159,7 +163,7 @@ def hbm_peak():
 
 
 def measure(app, steps=50, warmup=5, device=None, graph=True, warm=False,
-            cp=None):
+            cp=None, size=None):
     """Mean device time of ``steps`` runs of one shipped pipeline at its
     benchmark size (CUDA events on the launching stream).  By default 256 MB
     are written before each run so that nothing starts in L2; ``warm``
@@ -169,7 +173,7 @@ def measure(app, steps=50, warmup=5, device=None, graph=True, warm=False,
     import torch
     dev = device or torch.device("cuda", torch.cuda.current_device())
     cp = cp or catalog.build(app)
-    prm, host_in, out_spec, pixels, desc = workload(app)
+    prm, host_in, out_spec, pixels, desc = workload(app, size=size)
     # inputs that only const tables read (the camera pipe's two 3x4 colour
     # matrices) stay in host memory, where the tables are computed
     table_only = set(f.name for f in cp.inputs if id(f) in cp.table_only)
@@ -386,6 +390,9 @@ def main():
                          "(e.g. '[\"chain\"]')")
     ap.add_argument("--drop-options", default=None,
                     help="JSON list of catalog options left out")
+    ap.add_argument("--size", type=int, nargs=2, default=None,
+                    metavar=("ROWS", "COLS"),
+                    help="another image size (max filter only)")
     args = ap.parse_args()
     if args.int_peak:
         print(json.dumps(int_peak()))
@@ -400,13 +407,17 @@ def main():
             print(json.dumps(measure_host(app, min(args.steps, 20))))
         else:
             cp = None
-            add = [tuple(o) if isinstance(o, list) else o
-                   for o in json.loads(args.options or "[]")]
-            drop = [tuple(o) if isinstance(o, list) else o
-                    for o in json.loads(args.drop_options or "[]")]
+
+            def tup(o):
+                # JSON lists to the tuples options are written with, at
+                # every depth (('storage_order', (('vert', (3, 0, 1, 2)),)))
+                return tuple(tup(x) for x in o) if isinstance(o, list) else o
+            add = [tup(o) for o in json.loads(args.options or "[]")]
+            drop = [tup(o) for o in json.loads(args.drop_options or "[]")]
             if add or drop:
                 cp = catalog.variant(app, add, drop).build()
-            r = measure(app, args.steps, args.warmup, warm=args.warm, cp=cp)
+            r = measure(app, args.steps, args.warmup, warm=args.warm, cp=cp,
+                        size=tuple(args.size) if args.size else None)
             if add or drop:
                 r["options"] = add
                 r["dropped"] = drop
