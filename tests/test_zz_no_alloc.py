@@ -3,7 +3,10 @@ library, no allocation) against pm_mlp_forward (caller-provided activation
 buffer), through the C ABI.
 
 Both run the same kernels in the same order, so the outputs agree to
-max |static - buffered| <= 1e-6 * max(1, max |buffered|).  Requests beyond
+max |static - buffered| <= 1e-6 * max(1, max |buffered|); the static
+entry's output is also checked directly against the FP64 forward pass of
+oracle/mlp.py at the cost-model tests' tolerance (1e-4 relative to the
+largest output).  Requests beyond
 the array's 196,864 floats (B * (6H + 1)) return 1 and leave the output
 untouched.
 """
@@ -47,12 +50,17 @@ def test_static_forward_matches_buffered_forward(cuda):
     torch.cuda.synchronize()
     r = ref.cpu().numpy()
     tol = 1e-6 * max(1.0, float(np.abs(r).max()))
+    import oracle.mlp as OM
+    exact, _ = OM.forward(p.cpu().numpy(), X.cpu().numpy(), D, H)
     for _ in range(2):                       # two calls in a row
         out = torch.full((B,), -7.0, device=cuda)
         assert fwd_static(p.data_ptr(), D, H, X.data_ptr(), B,
                           out.data_ptr(), s) == 0
         torch.cuda.synchronize()
-        assert np.abs(out.cpu().numpy() - r).max() <= tol
+        o = out.cpu().numpy()
+        assert np.abs(o - r).max() <= tol
+        assert np.abs(o - exact).max() <= 1e-4 * max(1.0,
+                                                      np.abs(exact).max())
 
 
 def test_static_forward_rejects_oversized_request(cuda):
