@@ -372,6 +372,15 @@ def measure_stream(n=1024, seed=1, device=None):
             "l2": "inputs of each chunk (8 GB) larger than L2"}
 
 
+def parse_options(text):
+    """Build options from a JSON list: lists become the tuples options are
+    written with, at every depth (``[["storage_order", [["vert", [3, 0, 1,
+    2]]]]]`` is ``[('storage_order', (('vert', (3, 0, 1, 2)),))]``)."""
+    def tup(o):
+        return tuple(tup(x) for x in o) if isinstance(o, list) else o
+    return [tup(o) for o in json.loads(text or "[]")]
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--app", action="append",
@@ -407,13 +416,8 @@ def main():
             print(json.dumps(measure_host(app, min(args.steps, 20))))
         else:
             cp = None
-
-            def tup(o):
-                # JSON lists to the tuples options are written with, at
-                # every depth (('storage_order', (('vert', (3, 0, 1, 2)),)))
-                return tuple(tup(x) for x in o) if isinstance(o, list) else o
-            add = [tup(o) for o in json.loads(args.options or "[]")]
-            drop = [tup(o) for o in json.loads(args.drop_options or "[]")]
+            add = parse_options(args.options)
+            drop = parse_options(args.drop_options)
             if add or drop:
                 cp = catalog.variant(app, add, drop).build()
             r = measure(app, args.steps, args.warmup, warm=args.warm, cp=cp,

@@ -51,3 +51,20 @@ def test_timing_db_roundtrip_and_torn_line(tmp_path):
     assert len(rows) == 2
     t = relative_targets(rows)
     assert abs(t.sum()) < 1e-6 and t[0] > t[1]
+
+
+def test_measure_option_parsing_matches_catalog_options():
+    """measure --options / --drop-options: nested JSON lists become the
+    nested tuples the catalog writes, so a catalog option can be left out
+    by restating it."""
+    from polymage_b200.apps import catalog
+    from polymage_b200.apps.measure import parse_options
+    order = [o for o in catalog.MAXFILTER['options']
+             if isinstance(o, tuple) and o[0] == 'storage_order']
+    text = '[["storage_order",[["vert",[3,0,1,2]],["vert_log",[3,0,1,2]]]]]'
+    assert parse_options(text) == order
+    assert parse_options(None) == []
+    assert parse_options('["chain", "rblock=4"]') == ['chain', 'rblock=4']
+    p = catalog.variant("maxfilter", (), parse_options(text))
+    assert not any(isinstance(o, tuple) and o[0] == 'storage_order'
+                   for o in p.options)
