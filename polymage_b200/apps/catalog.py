@@ -45,7 +45,9 @@ is slower with that option), the L=8 pyramid and the local Laplacian with
 4 rows per thread (0.2164 vs 0.2237 ms, 0.1474 vs 0.1496 ms),
 interpolation with 3 resident CTAs (0.3048 vs 0.3138 ms).  Harris sums
 its 3x3 box sums and Sobel taps as row sums that the rows of a thread's
-block share (option separable: 0.0255 vs 0.0274 ms)."""
+block share (option separable: 0.0255 vs 0.0274 ms).  The 2-D multigrid
+cycles take 8x32 tiles: their 255^2 grids give 16x64 tiles too few CTAs
+for 148 SMs (V-cycle 0.061 vs 0.075 ms, W-cycle 0.113 vs 0.140 ms)."""
 
 import functools
 
@@ -97,7 +99,7 @@ JACOBI2D = dict(N=2048, T=10, tile_sizes=(32, 64), group_size=5,
                 options=('stage_pointwise',))
 JACOBI3D = dict(N=128, T=10, tile_sizes=(8, 16, 32), group_size=1,
                 options=('stage_pointwise',))
-VCYCLE = dict(n=31, L=3, nu1=10, nu2=0, nuc=0, tile_sizes=(16, 64),
+VCYCLE = dict(n=31, L=3, nu1=10, nu2=0, nuc=0, tile_sizes=(8, 32),
               group_size=6, options=('stage_pointwise',))
 WCYCLE = dict(VCYCLE, gamma=2, name="Wcycle")
 VCYCLE3D = dict(n=31, L=3, nu1=10, nu2=0, nuc=0, dims=3,
