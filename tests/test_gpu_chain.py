@@ -89,7 +89,6 @@ def test_chain_graph_replays_and_batch(cuda):
     import torch
     cp = _chain("pyramid8")
     R, C = 300, 420
-    outs = []
     for seed in (5, 6):
         img1, img2, mask = OP.make_inputs(R, C, seed=seed)
         ref = OP.pyramid_blend_clamped(img1, img2, mask, L=8)
@@ -103,7 +102,6 @@ def test_chain_graph_replays_and_batch(cuda):
             cp.check()
             got = o.cpu().numpy().astype(np.float64)
             assert np.abs(got - ref).max() <= 2e-5
-        outs.append((img1, img2, mask, ref))
     sizes = [(R, C), (77, 130)]
     params, ins, bouts, refs = [], [], [], []
     for (r, c), s in zip(sizes, (8, 9)):
